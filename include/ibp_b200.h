@@ -1,0 +1,167 @@
+/*
+ * ibp_b200.h -- C ABI of the B200-native Invariant Bit Packing engine (libibp_b200.so).
+ *
+ * Plain pointers and sizes only.  Every entry point replaces one function of the
+ * reference's PyTorch extension `ibp_cuda` (src/ibp_api.cu:124-135); the comment on
+ * each gives the reference file:line it replaces.  A foreign-function binding
+ * (ctypes, cgo, JNI, N-API) binds these symbols directly; INTEGRATION.md shows one.
+ *
+ * Conventions
+ *  - dataset rows: `num_vecs` rows of `vec_size` words of `word_bytes` bytes, row stride
+ *    vec_size words, in device memory or in pinned (page-locked, mapped) host memory;
+ *    kernels read host rows zero-copy over PCIe.
+ *  - mask / bitval: `vec_size` words (k-means: num_clusters x vec_size), device memory.
+ *  - bitmask: int32 words, bit (i % 32) of word i / 32 set when row i is stored compressed.
+ *  - index arrays: int64, device memory.  An index outside [0, num_vecs) is not read: the
+ *    row is skipped and bit 0 of the call's device status word is set (ibp_read_status).
+ *  - `workspace`: caller-owned device scratch of at least the size the matching
+ *    *_workspace_size() returns (may be NULL when that size is 0).  No entry point
+ *    allocates device memory, so every call can be captured in a CUDA graph except
+ *    ibp_preprocess_kmeans with init_rows == NULL (host shuffle) and the condensed
+ *    compressor's size query (which the caller synchronises on).
+ *  - `stream`: a cudaStream_t (NULL = legacy default stream).  All work is enqueued on
+ *    it; no entry point synchronises the host unless stated.
+ *  - return value: IBP_OK or an error code; ibp_last_error() gives a message (per thread).
+ *    Nothing ever calls exit().
+ */
+#ifndef IBP_B200_H
+#define IBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *ibp_stream_t; /* same type as cudaStream_t */
+
+typedef enum {
+    IBP_OK = 0,
+    IBP_ERR_ARGUMENT = 1,   /* invalid sizes, word size, pointers */
+    IBP_ERR_WORKSPACE = 2,  /* workspace missing or smaller than *_workspace_size() */
+    IBP_ERR_CUDA = 3,       /* a CUDA runtime call or launch failed */
+    IBP_ERR_UNSUPPORTED = 4 /* option the engine does not provide */
+} ibp_status;
+
+/* Message describing the last error returned on this thread ("" if none). */
+const char *ibp_last_error(void);
+
+/* ABI version of this header (bumped on any signature change). */
+int ibp_abi_version(void);
+
+/* Debug prints to stdout; replaces print_debug (src/ibp_api.cu:7-12). */
+void ibp_set_debug(int on);
+
+/* Profiling hooks (benchmarks): while set, every decompress_fetch on this thread records
+ * start_event (a cudaEvent_t) just before and stop_event just after its row-fetch kernel, on
+ * the call's stream.  NULL, NULL turns this off. */
+void ibp_set_profile_events(void *start_event, void *stop_event);
+
+/* Number of engine kernels this process has launched so far (all threads). */
+unsigned long long ibp_kernel_launch_count(void);
+
+/* Device status word of the last call that used `workspace`: bit 0 = an index was out of
+ * range.  Enqueues a copy on `stream` and waits for it (blocking). */
+ibp_status ibp_read_status(const void *workspace, int32_t *status, ibp_stream_t stream);
+
+/* ---------------------------------------------------------------- preprocess
+ * Replaces preprocess (src/preprocess.cu:17-76; include/preproc/ibp_preproc_host.cuh:23-115).
+ * threshold < 0: sweep 0.7f..1.0f in float32 steps of 0.05 and keep the first threshold
+ * with the most saved bits; otherwise use `threshold`.  mask/bitval (vec_size words each)
+ * are fully written: zero when no threshold saves any bit.  word_bytes in {1,2,4,8}.
+ * Non-blocking (the reference blocks): the selection runs on the device.  A host-resident
+ * dataset is copied into the workspace during the census (so the second pass reads HBM)
+ * when workspace_bytes >= ibp_preprocess_workspace_size(...) + num_vecs*vec_size*word_bytes
+ * rounded up to 256. */
+size_t ibp_preprocess_workspace_size(int64_t num_vecs, int64_t vec_size, int word_bytes,
+                                     float threshold);
+ibp_status ibp_preprocess(const void *dataset, int64_t num_vecs, int64_t vec_size,
+                          int word_bytes, float threshold, void *mask, void *bitval,
+                          void *workspace, size_t workspace_bytes, ibp_stream_t stream);
+
+/* ---------------------------------------------------------------- preprocess_kmeans
+ * Replaces preprocess_kmeans (src/preprocess.cu:88-139; ibp_preproc_host.cuh:118-284).
+ * word_bytes in {4,8}.  Centroid 0 is row 0 and centroid i (1 <= i < min(C, num_vecs)) is
+ * row init_rows[i] (a host array of min(C, num_vecs) entries; entry 0 is ignored).  With
+ * init_rows == NULL the rows come from std::random_shuffle over 0..num_vecs-1, as in the
+ * reference (process rand() state; blocking).  10 assignment/update rounds, then per-
+ * cluster masks at threshold 1.0f (the value the reference's sweep leaves behind; its
+ * `threshold` argument has no effect).  Ties between centroids go to the highest id.
+ * masks/bitvals: num_clusters x vec_size words; clusters: num_vecs int32 (device or
+ * pinned host memory). */
+size_t ibp_preprocess_kmeans_workspace_size(int64_t num_vecs, int64_t vec_size,
+                                            int word_bytes, int32_t num_clusters);
+ibp_status ibp_preprocess_kmeans(const void *dataset, int64_t num_vecs, int64_t vec_size,
+                                 int word_bytes, int32_t num_clusters,
+                                 const int64_t *init_rows, void *masks, void *bitvals,
+                                 int32_t *clusters, void *workspace, size_t workspace_bytes,
+                                 ibp_stream_t stream);
+
+/* ---------------------------------------------------------------- get_compress_size
+ * Replaces get_compress_size (src/compress.cu:25-174; include/misc/ibp_misc_dev.cuh:19-46).
+ * sizes[i] = compressed bytes of row index[i] (or row i when index == NULL; then
+ * num_index is ignored and num_vecs rows are sized); a row whose index is out of range gets
+ * size 0.  `total` (nullable, device memory) is incremented by the sum of sizes.
+ * word_bytes in {1,2,4,8}.  sizes: device or pinned host memory. */
+ibp_status ibp_get_compress_size(const void *dataset, int64_t num_vecs, int64_t vec_size,
+                                 int word_bytes, const void *mask, const void *bitval,
+                                 const int64_t *index, int64_t num_index, int64_t *sizes,
+                                 int64_t *total, ibp_stream_t stream);
+
+/* ---------------------------------------------------------------- compress_inplace
+ * Replaces compress_inplace (src/compress.cu:176-236; include/compress/ibp_compress_host.cuh:7-27).
+ * Row i (i < nrows, nrows = index ? num_index : num_vecs) becomes the compressed form of
+ * source row index[i] (or i), zero padded to vec_size words, when that is strictly smaller;
+ * otherwise the raw source row.  bitmask ((nrows+31)/32 int32, device) is fully written.
+ * With an index, every source row is read before any row is written (the reference races
+ * there); that needs nrows*vec_size*word_bytes bytes of workspace.  word_bytes in {4,8}. */
+size_t ibp_compress_inplace_workspace_size(int64_t num_index, int64_t vec_size, int word_bytes,
+                                           int has_index);
+ibp_status ibp_compress_inplace(void *dataset, int64_t num_vecs, int64_t vec_size,
+                                int word_bytes, const void *mask, const void *bitval,
+                                const int64_t *index, int64_t num_index, int32_t *bitmask,
+                                void *workspace, size_t workspace_bytes, ibp_stream_t stream);
+
+/* ---------------------------------------------------------------- compress_condensed
+ * Replaces compress_condensed (src/compress.cu:238-313; ibp_compress_kernel.cuh:58-94).
+ * Step 1: ibp_condensed_offsets turns sizes (from ibp_get_compress_size, device memory)
+ * into inclusive byte offsets in place and writes the total to *total (device memory).
+ * Step 2: the caller allocates total bytes (zeroed) and calls ibp_compress_condensed,
+ * which writes row i's compressed form (or raw row) at byte offset offsets[i-1]
+ * (0 for row 0).  word_bytes in {4,8}. */
+size_t ibp_condensed_offsets_workspace_size(int64_t nrows);
+ibp_status ibp_condensed_offsets(int64_t *sizes_to_offsets, int64_t nrows, int64_t *total,
+                                 void *workspace, size_t workspace_bytes, ibp_stream_t stream);
+size_t ibp_compress_condensed_workspace_size(int64_t vec_size, int word_bytes);
+ibp_status ibp_compress_condensed(const void *dataset, int64_t num_vecs, int64_t vec_size,
+                                  int word_bytes, const void *mask, const void *bitval,
+                                  const int64_t *index, int64_t num_index,
+                                  const int64_t *offsets, void *out, void *workspace,
+                                  size_t workspace_bytes, ibp_stream_t stream);
+
+/* ---------------------------------------------------------------- decompress_fetch
+ * Replaces decompress_fetch (src/decompress.cu:10-156; include/decompress/).
+ * out row k (k < nrows, nrows = index ? num_index : num_vecs) = decompressed row index[k]
+ * (or k) of `comp`, the fixed-stride in-place-compressed rows (device or pinned host;
+ * pinned host rows are read zero-copy).  out: nrows x vec_size words in device or pinned
+ * host memory.  comp_len (words, <= 0: vec_size) is the caller's average compressed row
+ * length, a tuning hint only.  nblks / nthreads / impl follow the reference knobs:
+ * impl -1 auto, 0/1/5 decompress (the engine picks its own kernel shape), 2 = plain
+ * uncompressed gather of the stored rows (the reference's baseline); other values are
+ * IBP_ERR_UNSUPPORTED.  nblks/nthreads <= 0 pick defaults.  word_bytes in {4,8}.
+ * With an index, rows are fetched in sorted order and each distinct row is read once;
+ * repeats are copied on the device. */
+size_t ibp_decompress_fetch_workspace_size(int64_t num_index, int64_t vec_size, int word_bytes,
+                                           int has_index);
+ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_size,
+                                int word_bytes, const void *mask, const void *bitval,
+                                const int32_t *bitmask, const int64_t *index,
+                                int64_t num_index, int32_t comp_len, void *out, int32_t nblks,
+                                int32_t nthreads, int32_t impl, void *workspace,
+                                size_t workspace_bytes, ibp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IBP_B200_H */

@@ -1,0 +1,321 @@
+"""Drop-in mirror of the reference's compiled extension module `ibp_cuda`.
+
+Same function names, positional signatures, defaults, output placement and argument
+checks (with the reference's error messages, raised as RuntimeError like TORCH_CHECK) as
+src/ibp_api.cu:20-40 and :124-135; every computation is a call into libibp_b200.so through
+its C ABI (invariantbitpacking_b200/_capi.py).  torch provides device memory and the
+current stream only.
+
+Behavioural differences from the reference, all deliberate:
+  * preprocess and get_compress_size never block the host; decompress_fetch allocates its
+    output with torch.empty (every row is written) instead of torch.zeros;
+  * compress_inplace blocks only when the dataset is in host memory (the caller may read it
+    right away); the reference blocks always (cudaFree);
+  * an index array with compress_inplace reads every source row before any row is
+    overwritten (the reference races);
+  * get_compress_size's counter is updated whatever its dtype's size (the reference writes
+    a temporary copy when it is not int64);
+  * decompress_fetch rejects impl 3/4 (the reference's upper-bound stand-ins that do not
+    decompress) and ignores nblks/nthreads values that do not fit the engine's kernels;
+  * preprocess_kmeans breaks distance ties toward the highest centroid id (the reference
+    races) and accepts keyword-only `seed_rows` to fix the centroid seeds.
+"""
+import numpy as np
+import torch
+
+from . import _capi
+
+_lib = _capi.lib
+_check = _capi.check
+
+_INT_DTYPE = {1: torch.int8, 2: torch.int16, 4: torch.int32, 8: torch.int64}
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def _torch_check(cond, msg):
+    if not cond:
+        raise RuntimeError(msg)
+
+
+def _gpu_accessible(t):
+    return t.device.type == "cuda" or t.is_pinned()
+
+
+def _workspace(nbytes, device):
+    if nbytes == 0:
+        return None, 0
+    return torch.empty(int(nbytes), dtype=torch.uint8, device=device), int(nbytes)
+
+
+def _cuda_device(*tensors):
+    for t in tensors:
+        if t is not None and t.device.type == "cuda":
+            return t.device
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _stage_budget(nbytes, device):
+    """Stage a host-resident dataset in HBM when it takes at most half the free memory."""
+    try:
+        free, _ = torch.cuda.mem_get_info(device)
+    except Exception:
+        return False
+    return nbytes <= free // 2
+
+
+_debug = False
+
+
+def print_debug(flag):
+    """src/ibp_api.cu:9-12"""
+    global _debug
+    _debug = bool(flag)
+    _lib.ibp_set_debug(1 if flag else 0)
+
+
+def preprocess(dataset, threshold_=None):
+    """src/preprocess.cu:17-76 -> (mask, bitval) int tensors of vec_size words on CUDA."""
+    _torch_check(dataset.device.type == "cuda" or dataset.is_pinned(),
+                 "Input tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(dataset.dim() == 2, "Input tensor must be 2D [num_vecs x vec_size]")
+    wb = dataset.element_size()
+    _torch_check(wb in (1, 2, 4, 8), "Input tensor must be 1, 2, 4, or 8-byte datatype")
+    _torch_check(dataset.is_contiguous(), "Input tensor must be contiguous")
+    threshold = -1.0 if threshold_ is None else float(threshold_)
+    n, v = dataset.shape
+    dev = _cuda_device(dataset)
+    with torch.cuda.device(dev):
+        mask = torch.empty(v, dtype=_INT_DTYPE[wb], device=dev)
+        bitval = torch.empty(v, dtype=_INT_DTYPE[wb], device=dev)
+        need = _lib.ibp_preprocess_workspace_size(n, v, wb, threshold)
+        if dataset.device.type != "cuda" and _stage_budget(n * v * wb, dev):
+            need += (n * v * wb + 255) // 256 * 256
+        ws, wsb = _workspace(need, dev)
+        _check(_lib.ibp_preprocess(_ptr(dataset), n, v, wb, threshold, _ptr(mask), _ptr(bitval),
+                                   _ptr(ws), wsb, _stream()))
+    return mask, bitval
+
+
+def preprocess_kmeans(dataset, num_clusters, threshold_=None, *, seed_rows=None):
+    """src/preprocess.cu:88-139 -> (mask[C,V], bitval[C,V] on CUDA, clusters int32 pinned)."""
+    _torch_check(dataset.device.type == "cuda" or dataset.is_pinned(),
+                 "Input tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(dataset.dim() == 2, "Input tensor must be 2D [num_vecs x vec_size]")
+    wb = dataset.element_size()
+    _torch_check(wb in (4, 8), "Input tensor must be 4-byte or 8-byte datatype")
+    _torch_check(dataset.is_contiguous(), "Input tensor must be contiguous")
+    c = int(num_clusters)
+    n, v = dataset.shape
+    dev = _cuda_device(dataset)
+    with torch.cuda.device(dev):
+        masks = torch.empty((c, v), dtype=_INT_DTYPE[wb], device=dev)
+        bitvals = torch.empty((c, v), dtype=_INT_DTYPE[wb], device=dev)
+        clusters = torch.zeros(n, dtype=torch.int32).pin_memory()
+        need = _lib.ibp_preprocess_kmeans_workspace_size(n, v, wb, c)
+        if dataset.device.type != "cuda" and _stage_budget(n * v * wb, dev):
+            need += (n * v * wb + 255) // 256 * 256
+        ws, wsb = _workspace(need, dev)
+        seeds = None
+        if seed_rows is not None:
+            seeds = np.ascontiguousarray(np.asarray(seed_rows, dtype=np.int64))
+        _check(_lib.ibp_preprocess_kmeans(
+            _ptr(dataset), n, v, wb, c,
+            None if seeds is None else seeds.ctypes.data, _ptr(masks), _ptr(bitvals),
+            _ptr(clusters), _ptr(ws), wsb, _stream()))
+        # the reference returns after cudaDeviceSynchronize; clusters is a host tensor
+        torch.cuda.current_stream().synchronize()
+    return masks, bitvals, clusters
+
+
+def _index_arg(index_array_, what="Index array"):
+    if index_array_ is None:
+        return None
+    idx = index_array_
+    _torch_check(idx.device.type == "cuda" or idx.is_pinned(),
+                 f"{what} must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(idx.dim() == 1, "Index array should be 1D")
+    return idx.to(torch.int64).contiguous()
+
+
+def _codec_checks(dataset, mask, bitval, codec_only):
+    _torch_check(dataset.device.type == "cuda" or dataset.is_pinned(),
+                 "Input tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(dataset.dim() in (1, 2),
+                 "Input tensor must be 1D [vec_size] or 2D [num_vecs x vec_size]")
+    _torch_check(dataset.is_contiguous(), "Input tensor must be contiguous")
+    _torch_check(_gpu_accessible(mask),
+                 "Mask tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(_gpu_accessible(bitval),
+                 "Bitval tensor must accessible by CUDA device (GPU or pinned memory)")
+    wb = dataset.element_size()
+    if codec_only:
+        _torch_check(wb in (4, 8), "Input tensor must be 4-byte or 8-byte datatype")
+    else:
+        _torch_check(wb in (1, 2, 4, 8), "Input tensor must be 1, 2, 4, or 8-byte datatype")
+    _torch_check(mask.element_size() == wb and bitval.element_size() == wb,
+                 "Mask and bitval tensors must have the same datatype size (4-byte or 8-byte) "
+                 "as input dataset")
+    n = 1 if dataset.dim() == 1 else dataset.shape[0]
+    v = dataset.shape[0] if dataset.dim() == 1 else dataset.shape[1]
+    return n, v, wb
+
+
+def get_compress_size(dataset, mask, bitval, index_array_=None, compress_ctr_=None):
+    """src/compress.cu:25-174 -> int64 compressed bytes per row (non-blocking)."""
+    n, v, wb = _codec_checks(dataset, mask, bitval, codec_only=False)
+    idx = _index_arg(index_array_)
+    nrows = n if idx is None else idx.shape[0]
+    ctr = None
+    if compress_ctr_ is not None:
+        ctr = compress_ctr_
+        _torch_check(ctr.device.type == "cuda" or ctr.is_pinned(),
+                     "Compress ctr must accessible by CUDA device (GPU or pinned memory)")
+        _torch_check(ctr.dim() == 1 and ctr.shape[0] == 1, "Compress ctr should be a single element")
+    dev = _cuda_device(dataset, mask, idx)
+    with torch.cuda.device(dev):
+        sizes = torch.empty(nrows, dtype=torch.int64, device=dataset.device)
+        if dataset.device.type != "cuda":
+            sizes = sizes.pin_memory()
+        total = None
+        if ctr is not None:
+            total = ctr if (ctr.device.type == "cuda" and ctr.dtype == torch.int64) else \
+                ctr.to(device=dev, dtype=torch.int64, non_blocking=True)
+        _check(_lib.ibp_get_compress_size(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
+                                          _ptr(idx), nrows, _ptr(sizes), _ptr(total),
+                                          _stream()))
+        if ctr is not None and total is not ctr:
+            ctr.copy_(total, non_blocking=True)
+    return sizes
+
+
+def compress_inplace(dataset, mask, bitval, index_array_=None):
+    """src/compress.cu:176-236 -> int32 bitmask on CUDA; dataset rows rewritten in place."""
+    n, v, wb = _codec_checks(dataset, mask, bitval, codec_only=True)
+    idx = _index_arg(index_array_)
+    nrows = n if idx is None else idx.shape[0]
+    dev = _cuda_device(dataset, mask, idx)
+    with torch.cuda.device(dev):
+        bitmask = torch.zeros((nrows + 31) // 32, dtype=torch.int32, device=dev)
+        need = _lib.ibp_compress_inplace_workspace_size(nrows, v, wb, 0 if idx is None else 1)
+        ws, wsb = _workspace(need, dev)
+        _check(_lib.ibp_compress_inplace(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
+                                         _ptr(idx), nrows, _ptr(bitmask), _ptr(ws), wsb,
+                                         _stream()))
+        if dataset.device.type != "cuda":
+            torch.cuda.current_stream().synchronize()
+    return bitmask
+
+
+def compress_condensed(dataset, mask, bitval, index_array_=None):
+    """src/compress.cu:238-313 -> (condensed words, inclusive byte offsets int64)."""
+    n, v, wb = _codec_checks(dataset, mask, bitval, codec_only=True)
+    idx = _index_arg(index_array_)
+    nrows = n if idx is None else idx.shape[0]
+    dev = _cuda_device(dataset, mask, idx)
+    with torch.cuda.device(dev):
+        offs = torch.empty(nrows, dtype=torch.int64, device=dev)
+        total = torch.zeros(1, dtype=torch.int64, device=dev)
+        _check(_lib.ibp_get_compress_size(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
+                                          _ptr(idx), nrows, _ptr(offs), None, _stream()))
+        ws, wsb = _workspace(_lib.ibp_condensed_offsets_workspace_size(nrows), dev)
+        _check(_lib.ibp_condensed_offsets(_ptr(offs), nrows, _ptr(total), _ptr(ws), wsb,
+                                          _stream()))
+        nbytes = int(total.item())  # synchronises, as the reference does
+        comp = torch.zeros(nbytes // wb, dtype=dataset.dtype, device=dataset.device)
+        if dataset.device.type != "cuda":
+            comp = comp.pin_memory()
+        ws2, wsb2 = _workspace(_lib.ibp_compress_condensed_workspace_size(v, wb), dev)
+        _check(_lib.ibp_compress_condensed(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
+                                           _ptr(idx), nrows, _ptr(offs), _ptr(comp), _ptr(ws2),
+                                           wsb2, _stream()))
+        if dataset.device.type != "cuda":
+            offs = offs.to("cpu").pin_memory()
+            torch.cuda.current_stream().synchronize()
+    return comp, offs
+
+
+def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=None,
+                     index_array_=None, nblks_=None, nthreads_=None, impl_=None,
+                     output_tensor=None):
+    """src/decompress.cu:10-156 -> decompressed rows (non-blocking)."""
+    _torch_check(comp_dataset.device.type == "cuda" or comp_dataset.is_pinned(),
+                 "Input tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(comp_dataset.dim() in (1, 2),
+                 "Input tensor must be 1D [vec_size] or 2D [num_vecs x vec_size] got "
+                 f"{comp_dataset.dim()}")
+    _torch_check(comp_dataset.is_contiguous(), "Input tensor must be contiguous")
+    _torch_check(_gpu_accessible(mask),
+                 "Mask tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(_gpu_accessible(bitval),
+                 "Bitval tensor must accessible by CUDA device (GPU or pinned memory)")
+    wb = comp_dataset.element_size()
+    _torch_check(wb in (4, 8), "Input tensor must be 4-byte or 8-byte datatype")
+    _torch_check(mask.element_size() == wb and bitval.element_size() == wb,
+                 "Mask and bitval tensors must have the same datatype size (4-byte or 8-byte) "
+                 "as input dataset")
+    if bitmask.dtype != torch.int32:
+        raise RuntimeError(f"expected scalar type Int but found {bitmask.dtype}")
+    n = 1 if comp_dataset.dim() == 1 else comp_dataset.shape[0]
+    v = comp_dataset.shape[0] if comp_dataset.dim() == 1 else comp_dataset.shape[1]
+    out_device = torch.device(out_device)
+    idx = None
+    if index_array_ is not None:
+        _torch_check(index_array_.device.type == "cuda",
+                     "Index array must accessible by CUDA device (GPU or pinned memory)")
+        _torch_check(index_array_.dim() == 1, "Index array should be 1D")
+        idx = index_array_.to(torch.int64).contiguous()
+    nrows = n if idx is None else idx.shape[0]
+    impl = -1 if impl_ is None else int(impl_)
+    comp_len = v
+    if comp_len_ is not None and int(comp_len_) > 0:
+        comp_len = int(comp_len_)
+    if output_tensor is not None:
+        _torch_check(output_tensor.device == out_device,
+                     "Output tensor device does not match specified output device")
+        _torch_check(output_tensor.dtype == comp_dataset.dtype,
+                     "Output tensor dtype does not match input dataset dtype")
+        _torch_check(output_tensor.shape[0] == nrows and output_tensor.shape[1] == v,
+                     "Output tensor shape does not match expected decompressed shape")
+        out = output_tensor
+    else:
+        out = torch.empty((nrows, v), dtype=comp_dataset.dtype, device=out_device)
+    if out_device.type != "cuda" and not out.is_pinned():
+        out = out.pin_memory()
+    dev = _cuda_device(comp_dataset, mask, idx, out)
+    with torch.cuda.device(dev):
+        need = _lib.ibp_decompress_fetch_workspace_size(nrows, v, wb, 0 if idx is None else 1)
+        ws, wsb = _workspace(need, dev)
+        _check(_lib.ibp_decompress_fetch(
+            _ptr(comp_dataset), n, v, wb, _ptr(mask), _ptr(bitval), _ptr(bitmask), _ptr(idx),
+            nrows, comp_len, _ptr(out), -1 if nblks_ is None else int(nblks_),
+            -1 if nthreads_ is None else int(nthreads_), impl, _ptr(ws), wsb, _stream()))
+        if _debug and ws is not None:
+            st = torch.zeros(1, dtype=torch.int32)
+            import ctypes
+            _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), _stream()))
+            if int(st[0]) & 1:
+                print("[ibp] decompress_fetch: an index was out of range; its rows were skipped")
+    return out
+
+
+def read_shared(filename, shape, dtype):
+    """src/ibp_api.cu:52-122: file contents in a new shared-memory CPU tensor."""
+    t = torch.empty(list(shape), dtype=dtype).share_memory_()
+    nbytes = t.numel() * t.element_size()
+    buf = t.reshape(-1).view(torch.uint8).numpy() if nbytes else None
+    with open(filename, "rb") as f:
+        off = 0
+        chunk = 1 << 30
+        while off < nbytes:
+            got = f.readinto(memoryview(buf[off:off + chunk]))
+            if not got:
+                break
+            off += got
+    return t

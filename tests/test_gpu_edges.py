@@ -1,0 +1,219 @@
+"""GPU edge cases and full-size properties, checked against the CPU oracle (which the
+golden vectors pin to the reference): empty inputs, tiny and ragged rows, repeated and
+out-of-range indices, host outputs, the raw-gather knob, direct C-ABI calls, and
+bit-exact round trips at the benchmark sizes."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ibp():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import invariantbitpacking_b200 as m
+    return m
+
+
+def npy(t):
+    torch.cuda.synchronize()
+    return t.detach().cpu().numpy()
+
+
+def same(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def masked_rows(rng, n, v, wb, frac=0.6, flip=0.2):
+    W = 8 * wb
+    it = {4: np.int32, 8: np.int64}[wb]
+    ut = {4: np.uint32, 8: np.uint64}[wb]
+    bits = rng.random((v, W)) < frac
+    m = np.zeros(v, dtype=np.uint64)
+    for b in range(W):
+        m |= bits[:, b].astype(np.uint64) << np.uint64(b)
+    m = m.astype(ut)
+    base = rng.integers(0, 2**63, v, dtype=np.uint64).astype(ut) & m
+    noise = rng.integers(0, 2**63, (n, v), dtype=np.uint64).astype(ut)
+    data = (noise & ~m) | base
+    data = np.where(rng.random((n, v)) < flip, noise, data)
+    return data.view(it), m.view(it), base.view(it)
+
+
+@pytest.mark.parametrize("wb", [4, 8])
+@pytest.mark.parametrize("v", [1, 2, 3, 31, 32, 33, 200])
+def test_small_and_ragged_rows(ibp, oracle, wb, v):
+    rng = np.random.default_rng(100 * v + wb)
+    n = 301
+    d, m, b = masked_rows(rng, n, v, wb)
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    x = torch.from_numpy(d).pin_memory()
+    assert same(npy(ibp.get_compress_size(x, dm, db)), oracle.compress_size(d, m, b))
+    ocomp, obm = oracle.compress(d, m, b)
+    bm = ibp.compress_inplace(x, dm, db)
+    assert same(npy(bm), obm)
+    assert same(npy(x), ocomp.view(d.dtype))
+    idx = rng.integers(0, n, 777).astype(np.int64)
+    out = ibp.decompress_fetch(x, dm, db, bm, "cuda", None, torch.from_numpy(idx).cuda())
+    assert same(npy(out), d[idx])
+    out = ibp.decompress_fetch(x.cuda(), dm, db, bm, "cuda")
+    assert same(npy(out), d)
+
+
+def test_empty_inputs(ibp):
+    d = np.zeros((0, 64), dtype=np.int64)
+    x = torch.from_numpy(d).cuda()
+    m, b = ibp.preprocess(x, 0.9)
+    assert same(npy(m), np.zeros(64, np.int64))
+    assert npy(ibp.get_compress_size(x, m, b)).shape == (0,)
+    bm = ibp.compress_inplace(x, m, b)
+    assert npy(bm).shape == (0,)
+    out = ibp.decompress_fetch(x, m, b, bm, "cuda")
+    assert npy(out).shape == (0, 64)
+    rng = np.random.default_rng(1)
+    d2, m2, b2 = masked_rows(rng, 50, 64, 8)
+    y = torch.from_numpy(d2).pin_memory()
+    dm, db = torch.from_numpy(m2).cuda(), torch.from_numpy(b2).cuda()
+    bm2 = ibp.compress_inplace(y, dm, db)
+    out = ibp.decompress_fetch(y, dm, db, bm2, "cuda", None,
+                               torch.zeros(0, dtype=torch.int64, device="cuda"))
+    assert npy(out).shape == (0, 64)
+
+
+def test_preprocess_nothing_saved_gives_zero_mask(ibp):
+    rng = np.random.default_rng(5)
+    d = rng.integers(-2**63, 2**63 - 1, (64, 40), dtype=np.int64)
+    m, b = ibp.preprocess(torch.from_numpy(d).cuda(), None)
+    assert not npy(m).any() and not npy(b).any()
+
+
+def test_repeated_indices_and_host_output(ibp, oracle):
+    rng = np.random.default_rng(7)
+    d, m, b = masked_rows(rng, 1000, 64, 8, frac=0.7, flip=0.1)
+    x = torch.from_numpy(d).pin_memory()
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    bm = ibp.compress_inplace(x, dm, db)
+    hot = np.concatenate([np.full(5000, 17), np.full(300, 999), rng.integers(0, 1000, 4000)])
+    idx = rng.permutation(hot).astype(np.int64)
+    out = ibp.decompress_fetch(x, dm, db, bm, "cuda", None, torch.from_numpy(idx).cuda())
+    assert same(npy(out), d[idx])
+    out = ibp.decompress_fetch(x, dm, db, bm, "cpu", None, torch.from_numpy(idx[:100]).cuda())
+    torch.cuda.synchronize()
+    assert out.device.type == "cpu" and out.is_pinned()
+    assert same(out.numpy(), d[idx[:100]])
+    buf = torch.empty((100, 64), dtype=torch.int64, device="cuda")
+    out = ibp.decompress_fetch(x, dm, db, bm, "cuda", None,
+                               torch.from_numpy(idx[:100]).int().cuda(), None, None, None, buf)
+    assert out.data_ptr() == buf.data_ptr()
+    assert same(npy(buf), d[idx[:100]])
+    raw = ibp.decompress_fetch(x, dm, db, bm, "cuda", None, torch.from_numpy(idx[:64]).cuda(),
+                               None, None, 2)
+    assert same(npy(raw), npy(x)[idx[:64]])
+
+
+def test_bad_index_is_flagged_not_read(ibp):
+    """An out-of-range row index is skipped and reported through the status word."""
+    from invariantbitpacking_b200 import _capi
+    rng = np.random.default_rng(9)
+    d, m, b = masked_rows(rng, 100, 64, 8)
+    x = torch.from_numpy(d).pin_memory()
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    bm = ibp.compress_inplace(x, dm, db)
+    idx = torch.tensor([3, 100, -1, 5, 1 << 40], dtype=torch.int64, device="cuda")
+    out = torch.zeros((5, 64), dtype=torch.int64, device="cuda")
+    lib = _capi.lib
+    wsb = lib.ibp_decompress_fetch_workspace_size(5, 64, 8, 1)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _capi.check(lib.ibp_decompress_fetch(x.data_ptr(), 100, 64, 8, dm.data_ptr(), db.data_ptr(),
+                                         bm.data_ptr(), idx.data_ptr(), 5, -1, out.data_ptr(),
+                                         -1, -1, -1, ws.data_ptr(), wsb, st))
+    status = ctypes.c_int32(0)
+    _capi.check(lib.ibp_read_status(ws.data_ptr(), ctypes.byref(status), st))
+    assert status.value & 1
+    o = npy(out)
+    assert same(o[0], d[3]) and same(o[3], d[5])
+    assert not o[1].any() and not o[2].any() and not o[4].any()
+
+
+def test_capi_direct_matches_oracle(ibp, oracle):
+    """Plain pointers through the C ABI (no torch layer) on device buffers."""
+    from invariantbitpacking_b200 import _capi
+    lib = _capi.lib
+    rng = np.random.default_rng(21)
+    n, v = 4000, 96
+    d, m, b = masked_rows(rng, n, v, 4, frac=0.5, flip=0.3)
+    st = torch.cuda.current_stream().cuda_stream
+    x = torch.from_numpy(d).cuda()
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    bm = torch.empty((n + 31) // 32, dtype=torch.int32, device="cuda")
+    wsb = lib.ibp_compress_inplace_workspace_size(n, v, 4, 0)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    _capi.check(lib.ibp_compress_inplace(x.data_ptr(), n, v, 4, dm.data_ptr(), db.data_ptr(),
+                                         None, n, bm.data_ptr(), ws.data_ptr(), wsb, st))
+    ocomp, obm = oracle.compress(d, m, b)
+    assert same(npy(x), ocomp.view(np.int32)) and same(npy(bm), obm)
+    out = torch.empty((n, v), dtype=torch.int32, device="cuda")
+    wsb = lib.ibp_decompress_fetch_workspace_size(n, v, 4, 0)
+    ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+    _capi.check(lib.ibp_decompress_fetch(x.data_ptr(), n, v, 4, dm.data_ptr(), db.data_ptr(),
+                                         bm.data_ptr(), None, 0, -1, out.data_ptr(), -1, -1, -1,
+                                         ws.data_ptr(), wsb, st))
+    assert same(npy(out), d)
+
+
+def test_compress_with_index_reads_sources_first(ibp, oracle):
+    rng = np.random.default_rng(31)
+    d, m, b = masked_rows(rng, 500, 64, 8)
+    idx = rng.permutation(500)[:400].astype(np.int64)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    bm = ibp.compress_inplace(x, dm, db, torch.from_numpy(idx).cuda())
+    ocomp, obm = oracle.compress(d, m, b, idx)
+    got = npy(x)
+    assert same(npy(bm), obm)
+    assert same(got[:400], ocomp.view(np.int64))
+    assert same(got[400:], d[400:])
+
+
+def test_plain_small_full_size(ibp, oracle):
+    """16384 x 128 int64 rows: preprocess(0.9) -> compress -> fetch 2048 rows, vs oracle."""
+    from invariantbitpacking_b200 import synthetic
+    d, idx = synthetic.plain_small()
+    om, ob, _ = oracle.preprocess(d, 0.9)
+    x = torch.from_numpy(d).pin_memory()
+    m, b = ibp.preprocess(x, 0.9)
+    assert same(npy(m), om.view(np.int64)) and same(npy(b), ob.view(np.int64))
+    ocomp, obm = oracle.compress(d, om, ob)
+    bm = ibp.compress_inplace(x, m, b)
+    assert same(npy(bm), obm) and same(npy(x), ocomp.view(np.int64))
+    out = ibp.decompress_fetch(x, m, b, bm, "cuda", None, torch.from_numpy(idx).cuda())
+    assert same(npy(out), d[idx])
+
+
+def test_graph_features_full_size_round_trip(ibp, oracle):
+    """2.4M x 64 int64 rows (1.2 GB pinned): sweep preprocess, compress, and Zipf batches of
+    100k/200k/400k rows decompressed bit-exact; sizes checked against the oracle."""
+    from invariantbitpacking_b200 import synthetic
+    d = synthetic.graph_features()
+    x = torch.from_numpy(d).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    mm = npy(m)
+    assert mm.any(), "the sweep found no invariant bits"
+    sz = npy(ibp.get_compress_size(x, m, b))
+    samp = np.random.default_rng(0).integers(0, d.shape[0], 20000)
+    assert same(sz[samp], oracle.compress_size(d, mm, npy(b), samp))
+    comp_len = ibp.get_single_compress_len(x, m, b)
+    assert 0 < comp_len < 64
+    ref = torch.from_numpy(d).cuda()
+    bm = ibp.compress_inplace(x, m, b)
+    z = synthetic.Zipf(d.shape[0], 1.1, seed=12)
+    for k in (100_000, 200_000, 400_000):
+        idx = torch.from_numpy(z.sample(k)).cuda()
+        out = ibp.decompress_fetch(x, m, b, bm, "cuda", comp_len, idx)
+        assert torch.equal(out, ref[idx])
