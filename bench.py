@@ -305,18 +305,18 @@ def main():
     wsp = torch.empty(wsb, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
-    def engine_step(k, ev=None):
+    def engine_step(k, src=None):
         idx = batches_dev[k % len(batches_dev)]
-        if ev is not None:
-            lib.ibp_set_profile_events(ctypes.c_void_p(ev[0].cuda_event),
-                                       ctypes.c_void_p(ev[1].cuda_event))
         _capi.check(lib.ibp_decompress_fetch(
-            x.data_ptr(), args.rows, V, 8, m.data_ptr(), b.data_ptr(), bm.data_ptr(),
-            idx.data_ptr(), idx.shape[0], comp_len, out.data_ptr(), -1, -1, -1,
-            wsp.data_ptr(), wsb, stream.cuda_stream))
-        if ev is not None:
-            lib.ibp_set_profile_events(None, None)
+            (src if src is not None else x).data_ptr(), args.rows, V, 8, m.data_ptr(),
+            b.data_ptr(), bm.data_ptr(), idx.data_ptr(), idx.shape[0], comp_len,
+            out.data_ptr(), -1, -1, -1, wsp.data_ptr(), wsb, stream.cuda_stream))
         return idx.shape[0]
+
+    def kernel_ms(n):
+        buf = (ctypes.c_float * n)()
+        got = lib.ibp_profile_take(buf, n)
+        return [float(buf[i]) for i in range(got)]
 
     # correctness of the timed configuration before timing it
     for k in range(len(batches)):
@@ -328,24 +328,23 @@ def main():
     torch.cuda.synchronize()
 
     # ---- value: engine call, index resident on the device
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
     barrier(ws)
     torch.cuda.synchronize()
     l0 = lib.ibp_kernel_launch_count()
+    _capi.check(lib.ibp_profile_enable(args.steps))
     with Clocks(torch.cuda.current_device()) as clk:
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record()
         rows = 0
         for k in range(args.steps):
-            rows += engine_step(k, kev[k])
+            rows += engine_step(k)
         s1.record()
         s1.synchronize()
     launches = lib.ibp_kernel_launch_count() - l0
+    kms = kernel_ms(args.steps)
     ms = max_over_ranks(s0.elapsed_time(s1), ws)
     barrier(ws)
     value = rows * V * 8 * ws / ms / 1e6  # GB/s, all ranks
-    kms = [kev[k][0].elapsed_time(kev[k][1]) for k in range(args.steps)]
     kuniq = [uniq_bytes[k % len(batches)] for k in range(args.steps)]
     kall = [all_bytes[k % len(batches)] for k in range(args.steps)]
     fetch_gbs = sum(kuniq) / sum(kms) / 1e6
@@ -387,19 +386,12 @@ def main():
     except Exception:
         hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
     k400 = [i for i, bt in enumerate(batches) if len(bt) == 400_000][0]
-    idx = batches_dev[k400]
-    dms = []
-    for r in range(6):
-        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-        lib.ibp_set_profile_events(ctypes.c_void_p(ev[0].cuda_event), ctypes.c_void_p(ev[1].cuda_event))
-        _capi.check(lib.ibp_decompress_fetch(
-            xd.data_ptr(), args.rows, V, 8, m.data_ptr(), b.data_ptr(), bm.data_ptr(),
-            idx.data_ptr(), idx.shape[0], comp_len, out.data_ptr(), -1, -1, -1,
-            wsp.data_ptr(), wsb, stream.cuda_stream))
-        lib.ibp_set_profile_events(None, None)
-        ev[1].synchronize()
-        if r >= 2:
-            dms.append(ev[0].elapsed_time(ev[1]))
+    for r in range(2):
+        engine_step(k400, xd)
+    _capi.check(lib.ibp_profile_enable(4))
+    for r in range(4):
+        engine_step(k400, xd)
+    dms = kernel_ms(4)
     nuniq = len(np.unique(batches[k400]))
     hbm_bytes = uniq_bytes[k400] + nuniq * V * 8
     hbm_gbs = hbm_bytes / (sum(dms) / len(dms)) / 1e6

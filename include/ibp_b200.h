@@ -12,8 +12,10 @@
  *    kernels read host rows zero-copy over PCIe.
  *  - mask / bitval: `vec_size` words (k-means: num_clusters x vec_size), device memory.
  *  - bitmask: int32 words, bit (i % 32) of word i / 32 set when row i is stored compressed.
- *  - index arrays: int64, device memory.  An index outside [0, num_vecs) is not read: the
- *    row is skipped and bit 0 of the call's device status word is set (ibp_read_status).
+ *  - index arrays: int64, device memory, `num_index` entries; num_index < 0 means "no
+ *    index" (rows 0..num_vecs-1, the pointer is ignored).  An index outside [0, num_vecs) is
+ *    not read: the row is skipped and bit 0 of the call's device status word is set
+ *    (ibp_read_status).
  *  - `workspace`: caller-owned device scratch of at least the size the matching
  *    *_workspace_size() returns (may be NULL when that size is 0).  No entry point
  *    allocates device memory, so every call can be captured in a CUDA graph except
@@ -53,10 +55,12 @@ int ibp_abi_version(void);
 /* Debug prints to stdout; replaces print_debug (src/ibp_api.cu:7-12). */
 void ibp_set_debug(int on);
 
-/* Profiling hooks (benchmarks): while set, every decompress_fetch on this thread records
- * start_event (a cudaEvent_t) just before and stop_event just after its row-fetch kernel, on
- * the call's stream.  NULL, NULL turns this off. */
-void ibp_set_profile_events(void *start_event, void *stop_event);
+/* Profiling hooks (benchmarks): after ibp_profile_enable(cap), the next `cap` row-fetch
+ * kernel launches (decompress_fetch, any thread) are bracketed by CUDA events on their
+ * stream.  ibp_profile_take waits for them, writes their durations in milliseconds to ms[]
+ * (at most `capacity` entries), returns how many, and turns profiling off. */
+ibp_status ibp_profile_enable(int32_t capacity);
+int32_t ibp_profile_take(float *ms, int32_t capacity);
 
 /* Number of engine kernels this process has launched so far (all threads). */
 unsigned long long ibp_kernel_launch_count(void);
@@ -100,8 +104,8 @@ ibp_status ibp_preprocess_kmeans(const void *dataset, int64_t num_vecs, int64_t 
 
 /* ---------------------------------------------------------------- get_compress_size
  * Replaces get_compress_size (src/compress.cu:25-174; include/misc/ibp_misc_dev.cuh:19-46).
- * sizes[i] = compressed bytes of row index[i] (or row i when index == NULL; then
- * num_index is ignored and num_vecs rows are sized); a row whose index is out of range gets
+ * sizes[i] = compressed bytes of row index[i] (or row i when num_index < 0, then
+ * num_vecs rows are sized); a row whose index is out of range gets
  * size 0.  `total` (nullable, device memory) is incremented by the sum of sizes.
  * word_bytes in {1,2,4,8}.  sizes: device or pinned host memory. */
 ibp_status ibp_get_compress_size(const void *dataset, int64_t num_vecs, int64_t vec_size,
@@ -111,7 +115,7 @@ ibp_status ibp_get_compress_size(const void *dataset, int64_t num_vecs, int64_t 
 
 /* ---------------------------------------------------------------- compress_inplace
  * Replaces compress_inplace (src/compress.cu:176-236; include/compress/ibp_compress_host.cuh:7-27).
- * Row i (i < nrows, nrows = index ? num_index : num_vecs) becomes the compressed form of
+ * Row i (i < nrows, nrows = num_index >= 0 ? num_index : num_vecs) becomes the compressed form of
  * source row index[i] (or i), zero padded to vec_size words, when that is strictly smaller;
  * otherwise the raw source row.  bitmask ((nrows+31)/32 int32, device) is fully written.
  * With an index, every source row is read before any row is written (the reference races
@@ -142,7 +146,7 @@ ibp_status ibp_compress_condensed(const void *dataset, int64_t num_vecs, int64_t
 
 /* ---------------------------------------------------------------- decompress_fetch
  * Replaces decompress_fetch (src/decompress.cu:10-156; include/decompress/).
- * out row k (k < nrows, nrows = index ? num_index : num_vecs) = decompressed row index[k]
+ * out row k (k < nrows, nrows = num_index >= 0 ? num_index : num_vecs) = decompressed row index[k]
  * (or k) of `comp`, the fixed-stride in-place-compressed rows (device or pinned host;
  * pinned host rows are read zero-copy).  out: nrows x vec_size words in device or pinned
  * host memory.  comp_len (words, <= 0: vec_size) is the caller's average compressed row

@@ -28,7 +28,8 @@ SIGNATURES = {
     "ibp_abi_version": (_INT, []),
     "ibp_set_debug": (None, [_INT]),
     "ibp_read_status": (_INT, [_P, _P, _P]),
-    "ibp_set_profile_events": (None, [_P, _P]),
+    "ibp_profile_enable": (_INT, [_I32]),
+    "ibp_profile_take": (_I32, [_P, _I32]),
     "ibp_kernel_launch_count": (ctypes.c_ulonglong, []),
     "ibp_preprocess_workspace_size": (_SZ, [_I64, _I64, _INT, _F]),
     "ibp_preprocess": (_INT, [_P, _I64, _I64, _INT, _F, _P, _P, _P, _SZ, _P]),

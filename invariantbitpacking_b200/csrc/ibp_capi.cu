@@ -18,9 +18,30 @@ static thread_local std::string g_err;
 bool g_debug = false;
 std::atomic<unsigned long long> g_launches{0};
 
-ProfileEvents &profile_events() {
-    static thread_local ProfileEvents ev;
-    return ev;
+struct Profiler {
+    std::mutex mu;
+    int cap = 0, used = 0;
+    std::vector<cudaEvent_t> ev;  // 2 per slot
+};
+static Profiler &profiler() {
+    static Profiler p;
+    return p;
+}
+
+int profile_begin(cudaStream_t st) {
+    Profiler &p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    if (p.used >= p.cap) return -1;
+    const int slot = p.used++;
+    cudaEventRecord(p.ev[2 * slot], st);
+    return slot;
+}
+
+void profile_end(int slot, cudaStream_t st) {
+    if (slot < 0) return;
+    Profiler &p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    cudaEventRecord(p.ev[2 * slot + 1], st);
 }
 
 void set_error(const char *fmt, ...) {
@@ -110,10 +131,10 @@ size_t compress_inplace_workspace(int64_t nidx, int64_t v, int wb, bool has_inde
 template <typename U>
 static ibp_status compress_inplace_t(U *data, int64_t n, int64_t v, const U *mask,
                                      const U *bitval, const int64_t *index, int64_t nidx,
-                                     int32_t *bitmask, void *ws, size_t ws_bytes,
+                                     bool has_index, int32_t *bitmask, void *ws, size_t ws_bytes,
                                      cudaStream_t st) {
-    const int64_t nrows = index ? nidx : n;
-    const size_t need = compress_inplace_workspace(nidx, v, sizeof(U), index != nullptr);
+    const int64_t nrows = has_index ? nidx : n;
+    const size_t need = compress_inplace_workspace(nidx, v, sizeof(U), has_index);
     if (!ws || ws_bytes < need) {
         set_error("compress_inplace: workspace of %zu bytes is below the required %zu", ws_bytes,
                   need);
@@ -124,7 +145,7 @@ static ibp_status compress_inplace_t(U *data, int64_t n, int64_t v, const U *mas
     ColTables<U> t = carve_tables<U>(c, v);
     IBP_CUDA(cudaMemsetAsync(status, 0, sizeof(int32_t), st));
     if (v > 0) IBP_RET(build_tables<U>(mask, bitval, v, t, st));
-    if (index) {
+    if (has_index) {
         // every source row is read before any row is overwritten
         U *stage = c.take<U>((size_t)(nidx * v));
         IBP_RET(gather_rows_impl<U>(data, n, v, index, nidx, stage, status, st));
@@ -146,9 +167,34 @@ int ibp_abi_version(void) { return 1; }
 
 void ibp_set_debug(int on) { g_debug = on != 0; }
 
-void ibp_set_profile_events(void *start_event, void *stop_event) {
-    profile_events().start = (cudaEvent_t)start_event;
-    profile_events().stop = (cudaEvent_t)stop_event;
+ibp_status ibp_profile_enable(int32_t capacity) {
+    clear_error();
+    Profiler &p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    IBP_ARG(capacity >= 0 && capacity <= (1 << 20), "profile_enable: bad capacity %d", capacity);
+    while ((int)p.ev.size() < 2 * capacity) {
+        cudaEvent_t e;
+        IBP_CUDA(cudaEventCreate(&e));
+        p.ev.push_back(e);
+    }
+    p.cap = capacity;
+    p.used = 0;
+    return IBP_OK;
+}
+
+int32_t ibp_profile_take(float *ms, int32_t capacity) {
+    Profiler &p = profiler();
+    std::lock_guard<std::mutex> g(p.mu);
+    const int n = p.used < capacity ? p.used : capacity;
+    for (int i = 0; i < n; ++i) {
+        ms[i] = -1.0f;
+        if (cudaEventSynchronize(p.ev[2 * i + 1]) == cudaSuccess)
+            cudaEventElapsedTime(&ms[i], p.ev[2 * i], p.ev[2 * i + 1]);
+    }
+    cudaGetLastError();
+    p.used = 0;
+    p.cap = 0;
+    return n;
 }
 
 unsigned long long ibp_kernel_launch_count(void) { return g_launches.load(); }
@@ -252,8 +298,9 @@ ibp_status ibp_get_compress_size(const void *dataset, int64_t num_vecs, int64_t 
                                  int64_t *total, ibp_stream_t stream) {
     clear_error();
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, false, "get_compress_size"));
-    const int64_t nrows = index ? num_index : num_vecs;
-    IBP_ARG(nrows >= 0, "get_compress_size: negative index length");
+    if (num_index < 0) index = nullptr;
+    const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
+    IBP_ARG(num_index <= 0 || index, "get_compress_size: null index array");
     IBP_ARG((mask && bitval) || vec_size == 0, "get_compress_size: null mask/bitval");
     IBP_ARG(sizes || nrows == 0, "get_compress_size: null sizes");
     IBP_ACCESSIBLE(mask, "get_compress_size", "mask");
@@ -296,9 +343,11 @@ ibp_status ibp_compress_inplace(void *dataset, int64_t num_vecs, int64_t vec_siz
                                 void *workspace, size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, true, "compress_inplace"));
-    const int64_t nrows = index ? num_index : num_vecs;
-    IBP_ARG(nrows >= 0, "compress_inplace: negative index length");
-    IBP_ARG(!index || num_index <= num_vecs,
+    if (num_index < 0) index = nullptr;
+    const bool has_index = num_index >= 0;
+    const int64_t nrows = has_index ? num_index : num_vecs;
+    IBP_ARG(num_index <= 0 || index, "compress_inplace: null index array");
+    IBP_ARG(!has_index || num_index <= num_vecs,
             "compress_inplace: %lld indexed rows do not fit a dataset of %lld rows",
             (long long)num_index, (long long)num_vecs);
     IBP_ARG((mask && bitval) || vec_size == 0, "compress_inplace: null mask/bitval");
@@ -311,11 +360,12 @@ ibp_status ibp_compress_inplace(void *dataset, int64_t num_vecs, int64_t vec_siz
     if (word_bytes == 4)
         return compress_inplace_t<uint32_t>((uint32_t *)dataset, num_vecs, vec_size,
                                             (const uint32_t *)mask, (const uint32_t *)bitval,
-                                            index, num_index, bitmask, workspace,
+                                            index, num_index, has_index, bitmask, workspace,
                                             workspace_bytes, st);
     return compress_inplace_t<uint64_t>((uint64_t *)dataset, num_vecs, vec_size,
                                         (const uint64_t *)mask, (const uint64_t *)bitval, index,
-                                        num_index, bitmask, workspace, workspace_bytes, st);
+                                        num_index, has_index, bitmask, workspace,
+                                        workspace_bytes, st);
 }
 
 // ------------------------------------------------------------------ compress_condensed
@@ -344,8 +394,9 @@ ibp_status ibp_compress_condensed(const void *dataset, int64_t num_vecs, int64_t
                                   size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, true, "compress_condensed"));
-    const int64_t nrows = index ? num_index : num_vecs;
-    IBP_ARG(nrows >= 0, "compress_condensed: negative index length");
+    if (num_index < 0) index = nullptr;
+    const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
+    IBP_ARG(num_index <= 0 || index, "compress_condensed: null index array");
     IBP_ARG((offsets && out) || nrows == 0, "compress_condensed: null offsets/out");
     IBP_ACCESSIBLE(mask, "compress_condensed", "mask");
     IBP_ACCESSIBLE(bitval, "compress_condensed", "bitval");
@@ -393,8 +444,9 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                 size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
     IBP_RET(check_rows(comp, num_vecs, vec_size, word_bytes, true, "decompress_fetch"));
-    const int64_t nrows = index ? num_index : num_vecs;
-    IBP_ARG(nrows >= 0, "decompress_fetch: negative index length");
+    if (num_index < 0) index = nullptr;
+    const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
+    IBP_ARG(num_index <= 0 || index, "decompress_fetch: null index array");
     IBP_ARG(out || nrows * vec_size == 0, "decompress_fetch: null output");
     if (impl != -1 && impl != 0 && impl != 1 && impl != 2 && impl != 5) {
         set_error("decompress_fetch: impl %d is not provided (3/4 are the reference's "
@@ -412,11 +464,13 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
     if (word_bytes == 4)
         return decompress_impl<uint32_t>((const uint32_t *)comp, num_vecs, vec_size,
                                          (const uint32_t *)mask, (const uint32_t *)bitval,
-                                         bitmask, index, num_index, comp_len, (uint32_t *)out,
+                                         bitmask, index, num_index, num_index >= 0, comp_len,
+                                         (uint32_t *)out,
                                          nblks, nthreads, impl, workspace, workspace_bytes, st);
     return decompress_impl<uint64_t>((const uint64_t *)comp, num_vecs, vec_size,
                                      (const uint64_t *)mask, (const uint64_t *)bitval, bitmask,
-                                     index, num_index, comp_len, (uint64_t *)out, nblks,
+                                     index, num_index, num_index >= 0, comp_len,
+                                     (uint64_t *)out, nblks,
                                      nthreads, impl, workspace, workspace_bytes, st);
 }
 

@@ -19,12 +19,10 @@ void clear_error();
 extern bool g_debug;
 extern std::atomic<unsigned long long> g_launches;  // engine kernels launched so far
 
-// Optional events recorded around the row-fetch kernel of the next decompress_fetch
-// (profiling hook for the benchmark; per thread).
-struct ProfileEvents {
-    cudaEvent_t start = nullptr, stop = nullptr;
-};
-ProfileEvents &profile_events();
+// Optional CUDA events around row-fetch kernel launches (benchmark profiling hook):
+// profile_begin returns a slot (or -1 when profiling is off or full), profile_end closes it.
+int profile_begin(cudaStream_t st);
+void profile_end(int slot, cudaStream_t st);
 
 #define IBP_DPRINTF(...)                       \
     do {                                       \

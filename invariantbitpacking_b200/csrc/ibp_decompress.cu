@@ -38,6 +38,7 @@ struct FetchArgs {
     U *out;
     int32_t *status;
     int64_t slot_words;   // shared-memory words per warp
+    int64_t first_words;  // words of the first read of a compressed row
 };
 
 template <typename U>
@@ -73,6 +74,24 @@ __device__ __forceinline__ void decode_row_warp(const U *__restrict__ buf, int64
     }
 }
 
+// Warp copy of row words [w0, w1) from global (host-mapped or device) memory into the same
+// word positions of a shared-memory slot: 16-byte loads when the row is 16-byte aligned
+// (whole aligned blocks; a block straddling w0 rewrites words already loaded with the same
+// values), word loads otherwise.
+template <typename U>
+__device__ __forceinline__ void load_words(U *__restrict__ buf, const U *__restrict__ row,
+                                           int64_t w0, int64_t w1) {
+    const int lane = threadIdx.x & 31;
+    if ((((uintptr_t)row) & 15) == 0) {
+        constexpr int per16 = 16 / sizeof(U);
+        const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
+        uint4 *b4 = reinterpret_cast<uint4 *>(buf);
+        for (int64_t q = w0 / per16 + lane; q < (w1 + per16 - 1) / per16; q += 32) b4[q] = r4[q];
+    } else {
+        for (int64_t w = w0 + lane; w < w1; w += 32) buf[w] = row[w];
+    }
+}
+
 template <typename U>
 __global__ void __launch_bounds__(256) fetch_rows_kernel(FetchArgs<U> a) {
     constexpr int W = 8 * sizeof(U);
@@ -97,37 +116,19 @@ __global__ void __launch_bounds__(256) fetch_rows_kernel(FetchArgs<U> a) {
             warp_copy<U>(orow, row, v);
             continue;
         }
-        // bitmap words, then the exact stream length from the per-column bit counts
-        for (int64_t w = lane; w < a.mw; w += 32) buf[w] = row[w];
+        // first read: words [0, first) -- the bitmap plus as much of the stream as the
+        // caller's average-length hint predicts, in one request per row
+        const int64_t first = a.first_words;
+        load_words<U>(buf, row, 0, first);
         __syncwarp();
         const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
         uint32_t bits = 0;
         for (int64_t j = lane; j < v; j += 32)
             bits += ((units[j >> 5] >> (j & 31)) & 1u) ? (uint32_t)__ldg(&a.t.nb[j]) : (uint32_t)W;
         bits = __reduce_add_sync(0xffffffffu, bits);
-        const int64_t dw = (bits + W - 1) / W;
-        // stream words [mw, mw + dw): 16-byte loads when the row is 16-byte aligned
-        const int64_t end = a.mw + dw;
-        if ((((uintptr_t)row) & 15) == 0) {
-            constexpr int per16 = 16 / sizeof(U);
-            const int64_t q0 = a.mw / per16, q1 = (end + per16 - 1) / per16;
-            const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
-            uint4 *b4 = reinterpret_cast<uint4 *>(buf);
-            // the first 16-byte block may hold bitmap words too: keep the loaded bitmap
-            for (int64_t q = q0 + lane; q < q1; q += 32) {
-                const uint4 x = r4[q];
-                if (q * per16 >= a.mw) {
-                    b4[q] = x;
-                } else {
-                    const U *xs = reinterpret_cast<const U *>(&x);
-#pragma unroll
-                    for (int e = 0; e < per16; ++e)
-                        if (q * per16 + e >= a.mw) buf[q * per16 + e] = xs[e];
-                }
-            }
-        } else {
-            for (int64_t w = a.mw + lane; w < end; w += 32) buf[w] = row[w];
-        }
+        const int64_t end = a.mw + (bits + W - 1) / W;  // exact compressed words of the row
+        // second read, only for rows longer than the hint
+        if (end > first) load_words<U>(buf, row, first, end);
         // words past the stream read as zero (get_bits looks one word ahead; the loaded
         // value there never reaches an output bit, zeroing keeps the slot deterministic)
         __syncwarp();
@@ -237,22 +238,19 @@ static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStre
         const int64_t need = (a.nrows + threads / 32 - 1) / (threads / 32);
         if (blocks > need) blocks = need;
     }
-    ProfileEvents &pe = profile_events();
-    if (pe.start) IBP_CUDA(cudaEventRecord(pe.start, st));
+    const int slot = profile_begin(st);
     kern<<<(unsigned)blocks, threads, smem, st>>>(a);
     IBP_LAUNCHED("fetch_rows_kernel");
-    if (pe.stop) IBP_CUDA(cudaEventRecord(pe.stop, st));
+    profile_end(slot, st);
     return IBP_OK;
 }
 
 template <typename U>
 ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                            const U *bitval, const int32_t *bitmask, const int64_t *idx,
-                           int64_t nidx, int comp_len, U *out, int nblks, int nthreads,
-                           int impl, void *ws, size_t ws_bytes, cudaStream_t st) {
-    (void)comp_len;
+                           int64_t nidx, bool has_index, int comp_len, U *out, int nblks,
+                           int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st) {
     const int wb = sizeof(U);
-    const bool has_index = idx != nullptr;
     const int64_t nrows = has_index ? nidx : n;
     const size_t need = decompress_workspace(nidx, v, wb, has_index);
     if (!ws || ws_bytes < need) {
@@ -278,6 +276,15 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     a.raw_only = impl == 2;
     a.out = out;
     a.status = status;
+    // first read of a compressed row: the hint (average compressed words) plus one word,
+    // rounded up to whole 32-byte sectors; without a hint, the first 128 bytes
+    {
+        const int64_t sector = 32 / wb;
+        int64_t want = (comp_len > 0 && comp_len < v) ? (int64_t)comp_len + 1 : 128 / wb;
+        if (want < a.mw + 1) want = a.mw + 1;
+        want = (want + sector - 1) / sector * sector;
+        a.first_words = want < v ? want : v;
+    }
     if (!has_index) return launch_fetch<U>(a, nblks, nthreads, st);
 
     if (nidx > 0x7fffffffLL) {
@@ -317,13 +324,13 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
 
 template ibp_status decompress_impl<uint32_t>(const uint32_t *, int64_t, int64_t,
                                               const uint32_t *, const uint32_t *,
-                                              const int32_t *, const int64_t *, int64_t, int,
-                                              uint32_t *, int, int, int, void *, size_t,
+                                              const int32_t *, const int64_t *, int64_t, bool,
+                                              int, uint32_t *, int, int, int, void *, size_t,
                                               cudaStream_t);
 template ibp_status decompress_impl<uint64_t>(const uint64_t *, int64_t, int64_t,
                                               const uint64_t *, const uint64_t *,
-                                              const int32_t *, const int64_t *, int64_t, int,
-                                              uint64_t *, int, int, int, void *, size_t,
+                                              const int32_t *, const int64_t *, int64_t, bool,
+                                              int, uint64_t *, int, int, int, void *, size_t,
                                               cudaStream_t);
 
 }  // namespace ibp200

@@ -53,8 +53,8 @@ size_t decompress_workspace(int64_t nidx, int64_t v, int wb, bool has_index);
 template <typename U>
 ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                            const U *bitval, const int32_t *bitmask, const int64_t *idx,
-                           int64_t nidx, int comp_len, U *out, int nblks, int nthreads,
-                           int impl, void *ws, size_t ws_bytes, cudaStream_t st);
+                           int64_t nidx, bool has_index, int comp_len, U *out, int nblks,
+                           int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st);
 
 // ---- k-means (ibp_kmeans.cu)
 size_t kmeans_workspace(int64_t n, int64_t v, int wb, int c);

@@ -10,8 +10,9 @@
 //    reference's racy outcomes, see include/preproc/ibp_preproc_kmeans.cuh:139-146).
 //  * update: per-(cluster, word, bit) set counts.  A warp takes 32 rows (lane = row),
 //    forms one membership ballot per cluster and one ballot per bit, and adds
-//    popc(bit ballot & membership) into shared-memory counters (lane = cluster, so the
-//    adds are conflict-free); the reference issues one global atomic per set bit.
+//    popc(bit ballot & membership) into per-block shared-memory counters (lane = cluster:
+//    one shared atomic per (cluster, bit) per 32 rows, no bank conflicts); the reference
+//    issues one global atomic per set bit.
 //  * the counts of the last round are exactly those of the final assignment, so the
 //    final masks need no extra pass over the data.
 #include <algorithm>
@@ -112,7 +113,8 @@ cluster_bits_kernel(const U *__restrict__ data, int64_t n, int64_t v,
 #pragma unroll 8
                 for (int b = 0; b < W; ++b) {
                     const uint32_t bm = __ballot_sync(0xffffffffu, (x >> b) & 1);
-                    if (lane < lim && (bm & mine)) myc[kk * W + b] += __popc(bm & mine);
+                    // the block's warps share these counters: shared-memory atomics
+                    if (lane < lim && (bm & mine)) atomicAdd(&myc[kk * W + b], __popc(bm & mine));
                 }
             }
         }

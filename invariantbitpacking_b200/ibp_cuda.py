@@ -188,8 +188,8 @@ def get_compress_size(dataset, mask, bitval, index_array_=None, compress_ctr_=No
             total = ctr if (ctr.device.type == "cuda" and ctr.dtype == torch.int64) else \
                 ctr.to(device=dev, dtype=torch.int64, non_blocking=True)
         _check(_lib.ibp_get_compress_size(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
-                                          _ptr(idx), nrows, _ptr(sizes), _ptr(total),
-                                          _stream()))
+                                          _ptr(idx), -1 if idx is None else nrows, _ptr(sizes),
+                                          _ptr(total), _stream()))
         if ctr is not None and total is not ctr:
             ctr.copy_(total, non_blocking=True)
     return sizes
@@ -206,8 +206,8 @@ def compress_inplace(dataset, mask, bitval, index_array_=None):
         need = _lib.ibp_compress_inplace_workspace_size(nrows, v, wb, 0 if idx is None else 1)
         ws, wsb = _workspace(need, dev)
         _check(_lib.ibp_compress_inplace(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
-                                         _ptr(idx), nrows, _ptr(bitmask), _ptr(ws), wsb,
-                                         _stream()))
+                                         _ptr(idx), -1 if idx is None else nrows,
+                                         _ptr(bitmask), _ptr(ws), wsb, _stream()))
         if dataset.device.type != "cuda":
             torch.cuda.current_stream().synchronize()
     return bitmask
@@ -223,7 +223,8 @@ def compress_condensed(dataset, mask, bitval, index_array_=None):
         offs = torch.empty(nrows, dtype=torch.int64, device=dev)
         total = torch.zeros(1, dtype=torch.int64, device=dev)
         _check(_lib.ibp_get_compress_size(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
-                                          _ptr(idx), nrows, _ptr(offs), None, _stream()))
+                                          _ptr(idx), -1 if idx is None else nrows, _ptr(offs),
+                                          None, _stream()))
         ws, wsb = _workspace(_lib.ibp_condensed_offsets_workspace_size(nrows), dev)
         _check(_lib.ibp_condensed_offsets(_ptr(offs), nrows, _ptr(total), _ptr(ws), wsb,
                                           _stream()))
@@ -233,8 +234,8 @@ def compress_condensed(dataset, mask, bitval, index_array_=None):
             comp = comp.pin_memory()
         ws2, wsb2 = _workspace(_lib.ibp_compress_condensed_workspace_size(v, wb), dev)
         _check(_lib.ibp_compress_condensed(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
-                                           _ptr(idx), nrows, _ptr(offs), _ptr(comp), _ptr(ws2),
-                                           wsb2, _stream()))
+                                           _ptr(idx), -1 if idx is None else nrows, _ptr(offs),
+                                           _ptr(comp), _ptr(ws2), wsb2, _stream()))
         if dataset.device.type != "cuda":
             offs = offs.to("cpu").pin_memory()
             torch.cuda.current_stream().synchronize()
@@ -265,6 +266,8 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
     n = 1 if comp_dataset.dim() == 1 else comp_dataset.shape[0]
     v = comp_dataset.shape[0] if comp_dataset.dim() == 1 else comp_dataset.shape[1]
     out_device = torch.device(out_device)
+    if out_device.type == "cuda" and out_device.index is None:
+        out_device = torch.device("cuda", torch.cuda.current_device())
     idx = None
     if index_array_ is not None:
         _torch_check(index_array_.device.type == "cuda",
@@ -294,7 +297,8 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
         ws, wsb = _workspace(need, dev)
         _check(_lib.ibp_decompress_fetch(
             _ptr(comp_dataset), n, v, wb, _ptr(mask), _ptr(bitval), _ptr(bitmask), _ptr(idx),
-            nrows, comp_len, _ptr(out), -1 if nblks_ is None else int(nblks_),
+            -1 if idx is None else nrows, comp_len, _ptr(out),
+            -1 if nblks_ is None else int(nblks_),
             -1 if nthreads_ is None else int(nthreads_), impl, _ptr(ws), wsb, _stream()))
         if _debug and ws is not None:
             st = torch.zeros(1, dtype=torch.int32)

@@ -87,6 +87,12 @@ def _rows(data):
     return d, d.shape[0], d.shape[1], d.dtype.itemsize
 
 
+def _like(out, data):
+    """Return word arrays in the caller's dtype (so comparisons with the input are exact)."""
+    dt = np.asarray(data).dtype
+    return out.view(dt) if dt.itemsize == out.dtype.itemsize else out
+
+
 def _idx(idx):
     return None if idx is None else np.ascontiguousarray(np.asarray(idx, dtype=np.int64))
 
@@ -132,7 +138,7 @@ def preprocess(data, threshold=None):
     sel = lib().orc_preprocess(_p(d), n, v, wb, thr, _p(m), _p(b), _p(saved), _p(thrs),
                                ctypes.byref(ns))
     k = ns.value
-    return m, b, {"selected": sel, "saved": saved[:k].copy(), "thresholds": thrs[:k].copy()}
+    return _like(m, data), _like(b, data), {"selected": sel, "saved": saved[:k].copy(), "thresholds": thrs[:k].copy()}
 
 
 def compress_size(data, mask, bitval, idx=None):
@@ -153,7 +159,7 @@ def compress(data, mask, bitval, idx=None):
     bm = np.zeros((nout + 31) // 32, dtype=np.int32)
     lib().orc_compress(_p(d), n, v, wb, _p(words(mask)), _p(words(bitval)), _p(ix), nout,
                        _p(out), _p(bm))
-    return out, bm
+    return _like(out, data), bm
 
 
 def compress_condensed(data, mask, bitval, idx=None):
@@ -167,7 +173,7 @@ def compress_condensed(data, mask, bitval, idx=None):
     out = np.zeros(total // wb, dtype=d.dtype)
     lib().orc_compress_condensed(_p(d), n, v, wb, _p(words(mask)), _p(words(bitval)), _p(ix),
                                  nout, _p(offs), _p(out))
-    return out, offs
+    return _like(out, data), offs
 
 
 def decompress(comp, mask, bitval, bitmask, idx=None):
@@ -178,7 +184,7 @@ def decompress(comp, mask, bitval, bitmask, idx=None):
     bm = np.ascontiguousarray(np.asarray(bitmask).view(np.int32))
     lib().orc_decompress(_p(d), n, v, wb, _p(words(mask)), _p(words(bitval)), _p(bm), _p(ix),
                          nout, _p(out))
-    return out
+    return _like(out, comp)
 
 
 def kmeans_assign(data, centroids):
@@ -194,7 +200,7 @@ def kmeans_update(data, clusters, c):
     cent = np.zeros((c, v), dtype=d.dtype)
     lib().orc_kmeans_update(_p(d), n, v, wb, _p(np.ascontiguousarray(clusters, dtype=np.int32)),
                             c, _p(cent))
-    return cent
+    return _like(cent, data)
 
 
 def kmeans_masks(data, clusters, c, thr=1.0):
@@ -203,7 +209,7 @@ def kmeans_masks(data, clusters, c, thr=1.0):
     b = np.zeros((c, v), dtype=d.dtype)
     lib().orc_kmeans_masks(_p(d), n, v, wb, _p(np.ascontiguousarray(clusters, dtype=np.int32)),
                            c, float(thr), _p(m), _p(b))
-    return m, b
+    return _like(m, data), _like(b, data)
 
 
 def random_shuffle_init(n, c, reseed=True):
@@ -224,4 +230,4 @@ def preprocess_kmeans(data, c, init=None):
     b = np.zeros((c, v), dtype=d.dtype)
     cl = np.zeros(n, dtype=np.int32)
     lib().orc_preprocess_kmeans(_p(d), n, v, wb, c, _p(ix), _p(m), _p(b), _p(cl))
-    return m, b, cl
+    return _like(m, data), _like(b, data), cl

@@ -38,17 +38,17 @@ def test_argument_errors_are_status_codes():
     st = lib.ibp_preprocess(None, 10, 10, 3, 0.9, None, None, None, 0, None)
     assert st == _capi.IBP_ERR_ARGUMENT
     assert b"1, 2, 4, or 8-byte" in lib.ibp_last_error()
-    st = lib.ibp_decompress_fetch(None, 0, 0, 8, None, None, None, None, 0, -1, None, -1, -1, 3,
+    st = lib.ibp_decompress_fetch(None, 0, 0, 8, None, None, None, None, -1, -1, None, -1, -1, 3,
                                   None, 0, None)
     assert st == _capi.IBP_ERR_UNSUPPORTED
     assert b"impl 3" in lib.ibp_last_error()
-    st = lib.ibp_compress_inplace(None, 4, 4, 2, None, None, None, 0, None, None, 0, None)
+    st = lib.ibp_compress_inplace(None, 4, 4, 2, None, None, None, -1, None, None, 0, None)
     assert st == _capi.IBP_ERR_ARGUMENT
     assert b"4-byte or 8-byte" in lib.ibp_last_error()
     st = lib.ibp_preprocess_kmeans(None, 5, 4, 8, 0, None, None, None, None, None, 0, None)
     assert st == _capi.IBP_ERR_ARGUMENT
     with pytest.raises(RuntimeError, match="4-byte or 8-byte"):
-        _capi.check(lib.ibp_compress_inplace(None, 4, 4, 2, None, None, None, 0, None, None, 0,
+        _capi.check(lib.ibp_compress_inplace(None, 4, 4, 2, None, None, None, -1, None, None, 0,
                                              None))
 
 

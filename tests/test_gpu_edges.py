@@ -155,14 +155,14 @@ def test_capi_direct_matches_oracle(ibp, oracle):
     wsb = lib.ibp_compress_inplace_workspace_size(n, v, 4, 0)
     ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
     _capi.check(lib.ibp_compress_inplace(x.data_ptr(), n, v, 4, dm.data_ptr(), db.data_ptr(),
-                                         None, n, bm.data_ptr(), ws.data_ptr(), wsb, st))
+                                         None, -1, bm.data_ptr(), ws.data_ptr(), wsb, st))
     ocomp, obm = oracle.compress(d, m, b)
     assert same(npy(x), ocomp.view(np.int32)) and same(npy(bm), obm)
     out = torch.empty((n, v), dtype=torch.int32, device="cuda")
     wsb = lib.ibp_decompress_fetch_workspace_size(n, v, 4, 0)
     ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
     _capi.check(lib.ibp_decompress_fetch(x.data_ptr(), n, v, 4, dm.data_ptr(), db.data_ptr(),
-                                         bm.data_ptr(), None, 0, -1, out.data_ptr(), -1, -1, -1,
+                                         bm.data_ptr(), None, -1, -1, out.data_ptr(), -1, -1, -1,
                                          ws.data_ptr(), wsb, st))
     assert same(npy(out), d)
 
