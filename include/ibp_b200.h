@@ -165,6 +165,26 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                 int32_t nthreads, int32_t impl, void *workspace,
                                 size_t workspace_bytes, ibp_stream_t stream);
 
+/* ---------------------------------------------------------------- decompress_fetch, no allocation
+ * No counterpart in the reference.  For callers that cannot allocate device memory at all
+ * (a host framework that owns every device byte and offers no allocation hook, an allocator
+ * policy that forbids cudaMalloc on the request path, code that must not risk the implicit
+ * device synchronisation of cudaMalloc/cudaFree).  Same arguments and results as
+ * ibp_decompress_fetch without nblks/nthreads/impl/workspace; its scratch is a static 4 MiB
+ * (4194304-byte) device array that the library reserves on every device that loads it, until
+ * the process exits.  A call that needs more scratch than that
+ * (ibp_decompress_fetch_workspace_size(...) > 4194304; roughly: more than ~50k index entries
+ * of 8-byte words) returns IBP_ERR_WORKSPACE before launching anything.  The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress, with that device
+ * current): make that first call before any stream capture on the device.  All calls share
+ * the array, and calls whose GPU work overlaps (other streams, other threads) race on it:
+ * serialise them.  Nothing is allocated or freed. */
+ibp_status ibp_decompress_fetch_noalloc(const void *comp, int64_t num_vecs, int64_t vec_size,
+                                        int word_bytes, const void *mask, const void *bitval,
+                                        const int32_t *bitmask, const int64_t *index,
+                                        int64_t num_index, int32_t comp_len, void *out,
+                                        ibp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

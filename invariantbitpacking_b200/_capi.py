@@ -46,6 +46,8 @@ SIGNATURES = {
     "ibp_decompress_fetch_workspace_size": (_SZ, [_I64, _I64, _INT, _INT]),
     "ibp_decompress_fetch": (_INT, [_P, _I64, _I64, _INT, _P, _P, _P, _P, _I64, _I32, _P, _I32,
                                     _I32, _I32, _P, _SZ, _P]),
+    "ibp_decompress_fetch_noalloc": (_INT, [_P, _I64, _I64, _INT, _P, _P, _P, _P, _I64, _I32,
+                                            _P, _P]),
 }
 
 
