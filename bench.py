@@ -37,7 +37,7 @@ METRIC = "decompress_fetch delivered GB/s (graph features, Zipf 1.1 mini-batches
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--rows", type=int, default=ROWS)
@@ -93,7 +93,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -377,6 +377,30 @@ def main():
 
     pcie = measured_pcie_h2d(torch)
 
+    # ---- the same fetches of the uncompressed set (impl 2: plain zero-copy gather, same sort
+    # and repeat fill): what the batch costs without compression
+    raw = torch.from_numpy(d).pin_memory()
+
+    def raw_step(k):
+        idx = batches_dev[k % len(batches_dev)]
+        _capi.check(lib.ibp_decompress_fetch(
+            raw.data_ptr(), args.rows, V, 8, None, None, None, idx.data_ptr(), idx.shape[0],
+            -1, out.data_ptr(), -1, -1, 2, wsp.data_ptr(), wsb, stream.cuda_stream))
+        return idx.shape[0]
+
+    for k in range(args.warmup):
+        raw_step(k)
+    torch.cuda.synchronize()
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record()
+    rrows = 0
+    for k in range(args.steps):
+        rrows += raw_step(k)
+    r1.record()
+    r1.synchronize()
+    raw_gbs = rrows * V * 8 / r0.elapsed_time(r1) / 1e6
+    del raw
+
     # ---- device-resident variant of the same fetch (HBM roofline)
     xd = x.cuda()
     hbm = None
@@ -447,6 +471,10 @@ def main():
             "roofline_hbm": hbm,
             "cpu_baseline": cpu,
             "cpu_baseline_uncompressed_gather": gather,
+            "gpu_uncompressed_gather": {"value": round(raw_gbs, 3), "unit": "GB/s",
+                                        "what": "same batches, uncompressed pinned rows, "
+                                                "zero-copy gather (impl 2) with the same "
+                                                "sort and repeat fill"},
             "reference_gpu": ref_gpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),

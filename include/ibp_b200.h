@@ -66,7 +66,9 @@ int32_t ibp_profile_take(float *ms, int32_t capacity);
 unsigned long long ibp_kernel_launch_count(void);
 
 /* Device status word of the last call that used `workspace`: bit 0 = an index was out of
- * range.  Enqueues a copy on `stream` and waits for it (blocking). */
+ * range; bit 1 = a row marked compressed has a bitmap whose stream would not fit the row
+ * (the bitmask/mask do not belong to the data), and its output row was left untouched.
+ * Enqueues a copy on `stream` and waits for it (blocking). */
 ibp_status ibp_read_status(const void *workspace, int32_t *status, ibp_stream_t stream);
 
 /* ---------------------------------------------------------------- preprocess

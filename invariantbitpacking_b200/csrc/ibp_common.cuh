@@ -66,7 +66,8 @@ void profile_end(int slot, cudaStream_t st);
 // ------------------------------------------------------------------ sizes
 constexpr size_t kAlign = 256;          // every workspace carve starts 256-byte aligned
 constexpr size_t kStatusBytes = 256;    // head of every workspace: device status word(s)
-constexpr int32_t kStatusBadIndex = 1;  // bit 0: an index was out of range
+constexpr int32_t kStatusBadIndex = 1;    // bit 0: an index was out of range
+constexpr int32_t kStatusCorruptRow = 2;  // bit 1: a row's bitmap does not fit its mask
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
