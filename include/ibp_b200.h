@@ -167,6 +167,57 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                 int32_t nthreads, int32_t impl, void *workspace,
                                 size_t workspace_bytes, ibp_stream_t stream);
 
+/* ---------------------------------------------------------------- batched multi-set fetch
+ * No single counterpart in the reference, which fetches one tensor set per decompress_fetch
+ * call (src/decompress.cu:10-156) and whose callers issue one call per table or tensor.  Here
+ * one launch serves many requests -- (set, row list, output) -- across sets with different
+ * row lengths, masks and compression ratios:
+ *   1. describe the sets (same word size) and register them once: the registry is a device
+ *      buffer the caller owns (ibp_sets_registry_size bytes) holding every set's descriptor
+ *      and per-column tables; it stays valid as long as the sets' buffers do.  Registration
+ *      blocks until the registry is written.
+ *   2. put up to max_requests ibp_request records and their count in DEVICE memory and call
+ *      ibp_batch_fetch.  It reads both on the device, so a CUDA graph that captured the call
+ *      can be replayed after the caller rewrites the records (e.g. with a copy node).
+ * Out-of-range rows or set ids set bit 0 of the status word (first 4 bytes of the workspace).
+ * Rows are fetched as listed (no de-duplication inside a request). */
+typedef struct {
+    const void *comp;       /* compressed rows, device or pinned host memory */
+    int64_t num_vecs;
+    int64_t vec_size;       /* words per row */
+    const void *mask;       /* vec_size words, device memory */
+    const void *bitval;     /* vec_size words, device memory */
+    const int32_t *bitmask; /* (num_vecs+31)/32 words, device memory */
+    int32_t comp_len;       /* average compressed row length in words (hint); <= 0: none */
+    int32_t reserved;
+} ibp_set_desc;
+
+typedef struct {
+    int32_t set;            /* registered set */
+    int32_t reserved;
+    const int64_t *index;   /* `count` row numbers (device); NULL: rows first .. first+count-1 */
+    int64_t first;
+    int64_t count;
+    void *out;              /* count x vec_size words, device or pinned host memory */
+} ibp_request;
+
+size_t ibp_sets_registry_size(const ibp_set_desc *sets, int32_t nsets, int word_bytes);
+ibp_status ibp_sets_register(const ibp_set_desc *sets, int32_t nsets, int word_bytes,
+                             void *registry, size_t registry_bytes, ibp_stream_t stream);
+size_t ibp_batch_fetch_workspace_size(void);
+ibp_status ibp_batch_fetch(const void *registry, const ibp_request *requests,
+                           const int32_t *num_requests, int32_t max_requests, void *workspace,
+                           size_t workspace_bytes, ibp_stream_t stream);
+/* Times the batch on every candidate launch shape (threads per block {128, 256} x rows in
+ * flight per warp {1, 2, 4} x blocks per SM {all, 2, 1}), keeps the fastest for this
+ * registry's (word size, longest row, compression-ratio bucket, residency) for the rest of
+ * the process, and writes it to chosen[0..3] (threads, rows in flight, blocks per SM, index).
+ * Blocking; runs the batch ~55 times. */
+ibp_status ibp_batch_autotune(const void *registry, const ibp_request *requests,
+                              const int32_t *num_requests, int32_t max_requests,
+                              void *workspace, size_t workspace_bytes, int32_t *chosen,
+                              ibp_stream_t stream);
+
 /* ---------------------------------------------------------------- decompress_fetch, no allocation
  * No counterpart in the reference.  For callers that cannot allocate device memory at all
  * (a host framework that owns every device byte and offers no allocation hook, an allocator

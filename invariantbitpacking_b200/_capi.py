@@ -46,9 +46,26 @@ SIGNATURES = {
     "ibp_decompress_fetch_workspace_size": (_SZ, [_I64, _I64, _INT, _INT]),
     "ibp_decompress_fetch": (_INT, [_P, _I64, _I64, _INT, _P, _P, _P, _P, _I64, _I32, _P, _I32,
                                     _I32, _I32, _P, _SZ, _P]),
+    "ibp_sets_registry_size": (_SZ, [_P, _I32, _INT]),
+    "ibp_sets_register": (_INT, [_P, _I32, _INT, _P, _SZ, _P]),
+    "ibp_batch_fetch_workspace_size": (_SZ, []),
+    "ibp_batch_fetch": (_INT, [_P, _P, _P, _I32, _P, _SZ, _P]),
+    "ibp_batch_autotune": (_INT, [_P, _P, _P, _I32, _P, _SZ, _P, _P]),
     "ibp_decompress_fetch_noalloc": (_INT, [_P, _I64, _I64, _INT, _P, _P, _P, _P, _I64, _I32,
                                             _P, _P]),
 }
+
+
+class SetDesc(ctypes.Structure):
+    """ibp_set_desc"""
+    _fields_ = [("comp", _P), ("num_vecs", _I64), ("vec_size", _I64), ("mask", _P),
+                ("bitval", _P), ("bitmask", _P), ("comp_len", _I32), ("reserved", _I32)]
+
+
+class Request(ctypes.Structure):
+    """ibp_request (48 bytes, the layout the batch kernel reads from device memory)"""
+    _fields_ = [("set", _I32), ("reserved", _I32), ("index", _P), ("first", _I64),
+                ("count", _I64), ("out", _P)]
 
 
 class IBPError(RuntimeError):

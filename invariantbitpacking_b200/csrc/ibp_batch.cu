@@ -1,0 +1,406 @@
+// ibp_batch.cu -- batched multi-set fetch: one launch serves many (tensor set, row list)
+// requests, across sets with different row lengths, masks and compression ratios, with a
+// device-resident set registry and a device-resident request table so the launch can be
+// captured once in a CUDA graph and replayed with new requests.  Launch shape (threads per
+// block, rows in flight per warp, blocks per SM) comes from a per-process autotuner keyed by
+// (word size, longest row, compression-ratio bucket, host/device residency).
+//
+// The reference fetches one set per decompress_fetch call (src/decompress.cu:10-156); its
+// embedding-bag and decoder-layer callers issue one call per table or tensor.
+#include <cub/block/block_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "ibp_fetch.cuh"
+#include "ibp_internal.cuh"
+
+namespace ibp200 {
+
+constexpr int kBatchScanThreads = 256;
+
+// Device layout of a registry: header, then nsets RowSet<U>, then every set's tables.
+struct RegistryHeader {
+    int32_t nsets;
+    int32_t word_bytes;
+    int64_t max_v;
+    int32_t host_resident;   // set 0 lives in host memory
+    int32_t ratio_bucket;    // mean first-read fraction of the rows, in tenths
+};
+
+struct RequestDev {  // mirrors ibp_request
+    int32_t set;
+    int32_t reserved;
+    const int64_t *index;
+    int64_t first;
+    int64_t count;
+    void *out;
+};
+static_assert(sizeof(RequestDev) == sizeof(ibp_request), "request layout");
+
+template <typename U>
+struct BatchArgs {
+    const RowSet<U> *sets;
+    int32_t nsets;
+    const RequestDev *reqs;
+    const int32_t *nreq;
+    int32_t max_req;
+    unsigned long long *work;
+    int32_t *status;
+    int64_t slot_words;
+    int slots;
+};
+
+// Units of 32 rows: request r owns units [prefix[r], prefix[r+1]).
+template <typename U, int NC>
+__global__ void __launch_bounds__(256) batch_fetch_kernel(BatchArgs<U> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int64_t *prefix = reinterpret_cast<int64_t *>(smem);
+    U *slots = reinterpret_cast<U *>(smem + align_up(sizeof(int64_t) * (a.max_req + 1), 16)) +
+               (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
+    const int nreq = min(max(*a.nreq, 0), a.max_req);
+    // block-wide exclusive scan of the requests' unit counts
+    {
+        const int per = (nreq + blockDim.x - 1) / blockDim.x;
+        const int r0 = threadIdx.x * per;
+        int64_t sum = 0;
+        for (int r = r0; r < r0 + per && r < nreq; ++r) {
+            const int64_t cnt = a.reqs[r].count;
+            sum += cnt > 0 ? (cnt + 31) / 32 : 0;
+        }
+        typedef cub::BlockScan<int64_t, 256> Scan;
+        __shared__ typename Scan::TempStorage tmp;
+        int64_t excl = 0, total = 0;
+        Scan(tmp).ExclusiveSum(sum, excl, total);
+        for (int r = r0; r < r0 + per && r < nreq; ++r) {
+            prefix[r] = excl;
+            const int64_t cnt = a.reqs[r].count;
+            excl += cnt > 0 ? (cnt + 31) / 32 : 0;
+        }
+        if (threadIdx.x == 0) prefix[nreq] = total;
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const int64_t total_units = prefix[nreq];
+    LaneTables<U, NC> lt;
+    int cur_set = -1;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(a.work, 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if ((int64_t)u >= total_units) break;
+        // request owning unit u: the last r with prefix[r] <= u
+        int lo = 0, hi = nreq - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= (int64_t)u) lo = mid; else hi = mid - 1;
+        }
+        const RequestDev rq = a.reqs[lo];
+        const int64_t k = ((int64_t)u - prefix[lo]) * 32 + lane;
+        const bool set_ok = rq.set >= 0 && rq.set < a.nsets;
+        if (!set_ok) {
+            if (lane == 0) atomicOr(a.status, kStatusBadIndex);
+            continue;
+        }
+        const RowSet<U> &s = a.sets[rq.set];
+        if (NC > 0 && rq.set != cur_set) {
+            lt.load(s.t, s.v);
+            cur_set = rq.set;
+        }
+        const bool valid = k < rq.count;
+        const int64_t key = valid ? (rq.index ? rq.index[k] : rq.first + k) : -1;
+        const bool bad = valid && (key < 0 || key >= s.n);
+        if (bad) atomicOr(a.status, kStatusBadIndex);
+        const bool head = valid && !bad;
+        U *orow = reinterpret_cast<U *>(rq.out) + (head ? k : 0) * s.v;
+        const bool packed = head && ((__ldg(&s.bitmask[key >> 5]) >> (key & 31)) & 1);
+        fetch_heads<U, NC>(s, lt, slots, a.slots, a.slot_words, key, orow, head, packed,
+                           a.status);
+    }
+}
+
+// ------------------------------------------------------------------ registry
+static size_t tables_bytes_wb(int64_t v, int wb) {
+    return wb == 8 ? tables_bytes<uint64_t>(v) : tables_bytes<uint32_t>(v);
+}
+
+static size_t registry_bytes(const ibp_set_desc *sets, int nsets, int wb) {
+    Sizer s;
+    s.take<RegistryHeader>(1);
+    s.take<char>((size_t)nsets * (wb == 8 ? sizeof(RowSet<uint64_t>) : sizeof(RowSet<uint32_t>)));
+    for (int i = 0; i < nsets; ++i) s.take<char>(tables_bytes_wb(sets[i].vec_size, wb));
+    return s.total();
+}
+
+static bool host_memory(const void *p) {
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged;
+}
+
+// Host copies of registry headers, by registry address (written at registration, so a
+// batch call never reads the device header back).
+static std::mutex g_reg_mu;
+static std::map<const void *, RegistryHeader> g_reg_headers;
+
+template <typename U>
+static ibp_status register_sets(const ibp_set_desc *sets, int nsets, void *reg, size_t bytes,
+                                cudaStream_t st) {
+    const int wb = sizeof(U);
+    Carver c{(char *)reg, 0, bytes};
+    RegistryHeader *hdr = c.take<RegistryHeader>(1);
+    RowSet<U> *dsets = c.take<RowSet<U>>((size_t)nsets);
+    std::vector<RowSet<U>> hsets((size_t)nsets);
+    RegistryHeader h{};
+    h.nsets = nsets;
+    h.word_bytes = wb;
+    double ratio = 0;
+    for (int i = 0; i < nsets; ++i) {
+        const ibp_set_desc &d = sets[i];
+        RowSet<U> &s = hsets[(size_t)i];
+        s.comp = (const U *)d.comp;
+        s.n = d.num_vecs;
+        s.v = d.vec_size;
+        s.mw = meta_bytes(d.vec_size, wb) / wb;
+        s.first_words = first_read_words(d.vec_size, s.mw, wb, d.comp_len);
+        s.bitmask = d.bitmask;
+        s.t = carve_tables<U>(c, d.vec_size);
+        if (!s.t.nb) {
+            set_error("sets_register: registry of %zu bytes is too small", bytes);
+            return IBP_ERR_WORKSPACE;
+        }
+        h.max_v = std::max<int64_t>(h.max_v, d.vec_size);
+        ratio += d.vec_size > 0 ? (double)s.first_words / (double)d.vec_size : 1.0;
+        if (d.vec_size > 0) IBP_RET(build_tables<U>((const U *)d.mask, (const U *)d.bitval, d.vec_size, s.t, st));
+    }
+    h.host_resident = nsets > 0 && host_memory(sets[0].comp);
+    h.ratio_bucket = nsets > 0 ? (int)std::lround(10.0 * ratio / nsets) : 10;
+    IBP_CUDA(cudaMemcpyAsync(dsets, hsets.data(), sizeof(RowSet<U>) * nsets, cudaMemcpyHostToDevice, st));
+    IBP_CUDA(cudaMemcpyAsync(hdr, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    // the host copies above are pageable: make them complete before `hsets` goes away
+    IBP_CUDA(cudaStreamSynchronize(st));
+    std::lock_guard<std::mutex> g(g_reg_mu);
+    g_reg_headers[reg] = h;
+    return IBP_OK;
+}
+
+// ------------------------------------------------------------------ launch shapes
+struct Shape {
+    int threads = 256;   // threads per block
+    int slots = kRowsInFlight;
+    int occupancy = 0;   // blocks per SM (0: as many as fit)
+};
+
+struct ShapeKey {
+    int wb;
+    int64_t max_v;
+    int ratio_bucket;
+    int host;
+    bool operator<(const ShapeKey &o) const {
+        return std::tie(wb, max_v, ratio_bucket, host) <
+               std::tie(o.wb, o.max_v, o.ratio_bucket, o.host);
+    }
+};
+
+static std::mutex g_shape_mu;
+static std::map<ShapeKey, Shape> g_shapes;
+
+template <typename U, int NC>
+static ibp_status launch_batch_nc(BatchArgs<U> a, int64_t max_v, Shape sh, cudaStream_t st) {
+    const size_t slot_bytes = (size_t)a.slot_words * sizeof(U);
+    const size_t head = align_up(sizeof(int64_t) * (a.max_req + 1), 16);
+    int threads = sh.threads;
+    int slots = std::max(1, std::min(sh.slots, kRowsInFlight));
+    const int maxs = device_max_smem_optin();
+    while (slots > 1 && head + slot_bytes * slots * (threads / 32) > 96 * 1024) --slots;
+    while (threads > 32 && head + slot_bytes * slots * (threads / 32) > (size_t)maxs) threads -= 32;
+    const size_t smem = head + slot_bytes * slots * (threads / 32);
+    if ((int64_t)smem > maxs) {
+        set_error("batch_fetch: %d requests and rows of %lld words do not fit shared memory",
+                  a.max_req, (long long)max_v);
+        return IBP_ERR_UNSUPPORTED;
+    }
+    a.slots = slots;
+    auto kern = batch_fetch_kernel<U, NC>;
+    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    if (per_sm < 1) per_sm = 1;
+    if (sh.occupancy > 0 && sh.occupancy < per_sm) per_sm = sh.occupancy;
+    const int blocks = device_sm_count() * per_sm;
+    const int slot = profile_begin(st);
+    kern<<<blocks, threads, smem, st>>>(a);
+    IBP_LAUNCHED("batch_fetch_kernel");
+    profile_end(slot, st);
+    return IBP_OK;
+}
+
+template <typename U>
+static ibp_status launch_batch(const void *reg, const RegistryHeader &h, const RequestDev *reqs,
+                               const int32_t *nreq, int32_t max_req, void *ws, size_t ws_bytes,
+                               Shape sh, cudaStream_t st) {
+    Carver c{(char *)reg, 0, (size_t)-1};
+    c.take<RegistryHeader>(1);
+    const RowSet<U> *sets = c.take<RowSet<U>>((size_t)h.nsets);
+    int32_t *status = reinterpret_cast<int32_t *>(ws);
+    BatchArgs<U> a{};
+    a.sets = sets;
+    a.nsets = h.nsets;
+    a.reqs = reqs;
+    a.nreq = nreq;
+    a.max_req = max_req;
+    a.status = status;
+    a.work = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(ws) + 64);
+    a.slot_words = (int64_t)align_up((size_t)h.max_v + 2, 16 / sizeof(U));
+    (void)ws_bytes;
+    IBP_CUDA(cudaMemsetAsync(ws, 0, 128, st));
+    if (h.max_v > 64) return launch_batch_nc<U, 0>(a, h.max_v, sh, st);
+    if (h.max_v > 32) return launch_batch_nc<U, 2>(a, h.max_v, sh, st);
+    return launch_batch_nc<U, 1>(a, h.max_v, sh, st);
+}
+
+static ibp_status read_header(const void *reg, RegistryHeader &h) {
+    std::lock_guard<std::mutex> g(g_reg_mu);
+    auto it = g_reg_headers.find(reg);
+    if (it == g_reg_headers.end()) {
+        set_error("batch_fetch: %p is not a registry made by ibp_sets_register in this process",
+                  reg);
+        return IBP_ERR_ARGUMENT;
+    }
+    h = it->second;
+    return IBP_OK;
+}
+
+}  // namespace ibp200
+
+using namespace ibp200;
+
+extern "C" {
+
+size_t ibp_sets_registry_size(const ibp_set_desc *sets, int32_t nsets, int word_bytes) {
+    if (!sets || nsets < 0 || (word_bytes != 4 && word_bytes != 8)) return 0;
+    return registry_bytes(sets, nsets, word_bytes);
+}
+
+ibp_status ibp_sets_register(const ibp_set_desc *sets, int32_t nsets, int word_bytes,
+                             void *registry, size_t registry_bytes_, ibp_stream_t stream) {
+    clear_error();
+    IBP_ARG(sets && nsets > 0, "sets_register: no sets");
+    IBP_ARG(word_bytes == 4 || word_bytes == 8, "sets_register: word size must be 4 or 8 bytes");
+    IBP_ARG(registry, "sets_register: null registry");
+    for (int i = 0; i < nsets; ++i) {
+        const ibp_set_desc &d = sets[i];
+        IBP_ARG(d.num_vecs >= 0 && d.vec_size > 0, "sets_register: set %d has a bad shape", i);
+        IBP_ARG(d.comp && d.mask && d.bitval && d.bitmask, "sets_register: set %d has a null pointer", i);
+    }
+    const size_t need = registry_bytes(sets, nsets, word_bytes);
+    if (registry_bytes_ < need) {
+        set_error("sets_register: registry of %zu bytes is below the required %zu", registry_bytes_,
+                  need);
+        return IBP_ERR_WORKSPACE;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (word_bytes == 8) return register_sets<uint64_t>(sets, nsets, registry, registry_bytes_, st);
+    return register_sets<uint32_t>(sets, nsets, registry, registry_bytes_, st);
+}
+
+size_t ibp_batch_fetch_workspace_size(void) { return kStatusBytes; }
+
+ibp_status ibp_batch_fetch(const void *registry, const ibp_request *requests,
+                           const int32_t *num_requests, int32_t max_requests, void *workspace,
+                           size_t workspace_bytes, ibp_stream_t stream) {
+    clear_error();
+    IBP_ARG(registry && requests && num_requests, "batch_fetch: null registry/requests/count");
+    IBP_ARG(max_requests > 0 && max_requests <= 8192, "batch_fetch: max_requests must be 1..8192");
+    if (!workspace || workspace_bytes < kStatusBytes) {
+        set_error("batch_fetch: workspace of %zu bytes is below the required %zu", workspace_bytes,
+                  kStatusBytes);
+        return IBP_ERR_WORKSPACE;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    RegistryHeader h{};
+    IBP_RET(read_header(registry, h));
+    Shape sh;
+    {
+        std::lock_guard<std::mutex> g(g_shape_mu);
+        auto it = g_shapes.find(ShapeKey{h.word_bytes, h.max_v, h.ratio_bucket, h.host_resident});
+        if (it != g_shapes.end()) sh = it->second;
+    }
+    const RequestDev *reqs = reinterpret_cast<const RequestDev *>(requests);
+    if (h.word_bytes == 8)
+        return launch_batch<uint64_t>(registry, h, reqs, num_requests, max_requests, workspace,
+                                      workspace_bytes, sh, st);
+    return launch_batch<uint32_t>(registry, h, reqs, num_requests, max_requests, workspace,
+                                  workspace_bytes, sh, st);
+}
+
+ibp_status ibp_batch_autotune(const void *registry, const ibp_request *requests,
+                              const int32_t *num_requests, int32_t max_requests,
+                              void *workspace, size_t workspace_bytes, int32_t *chosen,
+                              ibp_stream_t stream) {
+    clear_error();
+    // warm up (and read the header) through the normal entry point
+    IBP_RET(ibp_batch_fetch(registry, requests, num_requests, max_requests, workspace,
+                            workspace_bytes, stream));
+    cudaStream_t st = (cudaStream_t)stream;
+    RegistryHeader h{};
+    IBP_RET(read_header(registry, h));
+    const ShapeKey key{h.word_bytes, h.max_v, h.ratio_bucket, h.host_resident};
+    std::vector<Shape> cands;
+    for (int threads : {128, 256})
+        for (int slots : {1, 2, 4})
+            for (int occ : {0, 2, 1}) cands.push_back(Shape{threads, slots, occ});
+    cudaEvent_t e0, e1;
+    IBP_CUDA(cudaEventCreate(&e0));
+    IBP_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    Shape best_sh;
+    int best_i = 0;
+    for (size_t i = 0; i < cands.size(); ++i) {
+        {
+            std::lock_guard<std::mutex> g(g_shape_mu);
+            g_shapes[key] = cands[i];
+        }
+        float tot = 0;
+        ibp_status s = IBP_OK;
+        for (int rep = 0; rep < 3 && s == IBP_OK; ++rep) {
+            cudaEventRecord(e0, st);
+            s = ibp_batch_fetch(registry, requests, num_requests, max_requests, workspace,
+                                workspace_bytes, stream);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) tot += ms;  // first run of a shape is a warm-up
+        }
+        if (s == IBP_OK && tot < best) {
+            best = tot;
+            best_sh = cands[i];
+            best_i = (int)i;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+        std::lock_guard<std::mutex> g(g_shape_mu);
+        g_shapes[key] = best_sh;
+    }
+    if (chosen) {
+        chosen[0] = best_sh.threads;
+        chosen[1] = best_sh.slots;
+        chosen[2] = best_sh.occupancy;
+        chosen[3] = best_i;
+    }
+    IBP_DPRINTF("[ibp] batch autotune: threads %d, rows in flight %d, blocks/SM %d (%.3f ms)\n",
+                best_sh.threads, best_sh.slots, best_sh.occupancy, best / 2);
+    return IBP_OK;
+}
+
+}  // extern "C"

@@ -25,19 +25,16 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include "ibp_codec.cuh"
+#include "ibp_fetch.cuh"
 #include "ibp_internal.cuh"
 
 namespace ibp200 {
 
 constexpr int kFetchThreads = 256;  // 8 warps per block
-constexpr int kRowsInFlight = 4;    // first reads a warp keeps outstanding
 
 template <typename U>
 struct FetchArgs {
-    const U *comp;
-    int64_t n, v, mw;
-    ColTables<U> t;
-    const int32_t *bitmask;
+    RowSet<U> s;
     const int64_t *keys;  // source rows in processing order (nullptr: position k is row k)
     const int64_t *pos;   // output row of each position (nullptr: k)
     int64_t nrows;
@@ -47,133 +44,8 @@ struct FetchArgs {
     int32_t *status;
     unsigned long long *work;  // chunk counter, zero at launch
     int64_t slot_words;   // shared-memory words per row slot
-    int64_t first_words;  // words of the first read of a compressed row
     int slots;            // row slots per warp (<= kRowsInFlight)
 };
-
-// Copy row words [w0, w1) into the same positions of a shared slot: 16-byte loads when the
-// row is 16-byte aligned (whole aligned blocks; a block straddling w0 rewrites words already
-// present with the same values), word loads otherwise.
-template <typename U>
-__device__ __forceinline__ void issue_words(U *__restrict__ slot, const U *__restrict__ row,
-                                            int64_t w0, int64_t w1) {
-    const int lane = threadIdx.x & 31;
-    if ((((uintptr_t)row) & 15) == 0) {
-        constexpr int per16 = 16 / sizeof(U);
-        const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
-        uint4 *b4 = reinterpret_cast<uint4 *>(slot);
-        for (int64_t q = w0 / per16 + lane; q < (w1 + per16 - 1) / per16; q += 32) b4[q] = r4[q];
-    } else {
-        for (int64_t w = w0 + lane; w < w1; w += 32) slot[w] = row[w];
-    }
-}
-
-// ------------------------------------------------------------------ column tables
-// Tables of the columns j = lane + 32*c, c < NC, held in registers (NC = 1 or 2), or read
-// through L1 from the workspace copy (NC = 0, any row length).
-template <typename U, int NC>
-struct LaneTables {
-    static constexpr int LW = LogW<U>::value;
-    U m[NC > 0 ? NC : 1], bv[NC > 0 ? NC : 1], mv[NC > 0 ? NC : 1][LW];
-    int nb[NC > 0 ? NC : 1];
-
-    __device__ __forceinline__ void load(const ColTables<U> &t, int64_t v) {
-        const int lane = threadIdx.x & 31;
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const int64_t j = lane + 32 * c;
-            const bool in = j < v;
-            m[c] = in ? t.mask[j] : (U)0;
-            bv[c] = in ? t.bitval[j] : (U)0;
-            nb[c] = in ? (int)t.nb[j] : 0;
-#pragma unroll
-            for (int i = 0; i < LW; ++i) mv[c][i] = in ? t.mv[i * v + j] : (U)0;
-        }
-    }
-};
-
-template <typename U>
-__device__ __forceinline__ U scatter_regs(U y, U sel, const U *mv) {
-    constexpr int LW = LogW<U>::value;
-#pragma unroll
-    for (int i = LW - 1; i >= 0; --i) {
-        const U t = (U)(y << (1 << i));
-        y = (U)((y & ~mv[i]) | (t & mv[i]));
-    }
-    return (U)(y & sel);
-}
-
-// Decode one compressed row from its shared-memory slot (bitmap at word 0, stream at word
-// mw, zero words after the stream) into the output row.
-template <typename U, int NC>
-__device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v, int64_t mw,
-                                           const ColTables<U> &t, const LaneTables<U, NC> &lt,
-                                           U *__restrict__ orow) {
-    constexpr int W = 8 * sizeof(U);
-    const int lane = threadIdx.x & 31;
-    const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
-    const U *stream = buf + mw;
-    int64_t base = 0;
-    auto chunk = [&](int64_t c0, U m, U bv, int nbits, const U *mv, int stride) {
-        const int64_t j = c0 + lane;
-        const bool in = j < v;
-        const bool cj = in && ((units[j >> 5] >> (j & 31)) & 1u);
-        const int L = in ? (cj ? nbits : W) : 0;
-        int incl = L;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (in) {
-            const U y = get_bits<U>(stream, base + incl - L, L);
-            U x = y;
-            if (cj) {
-                if (stride == 0)
-                    x = (U)(bv | scatter_regs<U>(y, (U)~m, mv));
-                else
-                    x = (U)(bv | scatter_bits<U>(y, (U)~m, mv, stride));
-            }
-            orow[j] = x;
-        }
-        base += __shfl_sync(0xffffffffu, incl, 31);
-    };
-    if constexpr (NC > 0) {
-#pragma unroll
-        for (int c = 0; c < NC; ++c)
-            if (32 * c < v) chunk(32 * c, lt.m[c], lt.bv[c], lt.nb[c], lt.mv[c], 0);
-    } else {
-        for (int64_t c0 = 0; c0 < v; c0 += 32) {
-            const int64_t j = c0 + lane;
-            const bool in = j < v;
-            chunk(c0, in ? __ldg(&t.mask[j]) : (U)0, in ? __ldg(&t.bitval[j]) : (U)0,
-                  in ? (int)__ldg(&t.nb[j]) : 0, t.mv + (in ? j : 0), (int)v);
-        }
-    }
-}
-
-// Exact compressed words of the row whose bitmap is in the slot (bitmap + stream).
-template <typename U, int NC>
-__device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t v, int64_t mw,
-                                             const ColTables<U> &t,
-                                             const LaneTables<U, NC> &lt) {
-    constexpr int W = 8 * sizeof(U);
-    const int lane = threadIdx.x & 31;
-    const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
-    uint32_t bits = 0;
-    if constexpr (NC > 0) {
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const int64_t j = lane + 32 * c;
-            if (j < v) bits += ((units[j >> 5] >> (j & 31)) & 1u) ? (uint32_t)lt.nb[c] : (uint32_t)W;
-        }
-    } else {
-        for (int64_t j = lane; j < v; j += 32)
-            bits += ((units[j >> 5] >> (j & 31)) & 1u) ? (uint32_t)__ldg(&t.nb[j]) : (uint32_t)W;
-    }
-    bits = __reduce_add_sync(0xffffffffu, bits);
-    return mw + (bits + W - 1) / W;
-}
 
 // ------------------------------------------------------------------ fetch kernel
 template <typename U, int NC>
@@ -181,9 +53,8 @@ __global__ void __launch_bounds__(kFetchThreads) fetch_rows_kernel(FetchArgs<U> 
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     U *slots = reinterpret_cast<U *>(smem) + (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
-    const int64_t v = a.v;
     LaneTables<U, NC> lt;
-    if (!a.raw_only) lt.load(a.t, v);
+    if (!a.raw_only) lt.load(a.s.t, a.s.v);
     for (;;) {
         unsigned long long chunk = 0;
         if (lane == 0) chunk = atomicAdd(a.work, 1ull);
@@ -200,95 +71,14 @@ __global__ void __launch_bounds__(kFetchThreads) fetch_rows_kernel(FetchArgs<U> 
             if (lane == 0) prev = k0 > 0 ? a.keys[k0 - 1] : key - 1;
             head = valid && key != prev;
         }
-        const bool bad = head && (key < 0 || key >= a.n);
+        const bool bad = head && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         head = head && !bad;
-        const int64_t dst = head ? (a.pos ? a.pos[k] : k) : 0;
+        U *orow = a.out + (head ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
         const bool packed =
-            head && !a.raw_only && ((__ldg(&a.bitmask[key >> 5]) >> (key & 31)) & 1);
-        unsigned hm = __ballot_sync(0xffffffffu, head);
-        while (hm) {
-            // up to `slots` heads: issue all their first reads, then decode them in turn
-            int lid[kRowsInFlight];
-            int cnt = 0;
-#pragma unroll
-            for (int s = 0; s < kRowsInFlight; ++s) {
-                lid[s] = 0;
-                if (s < a.slots && hm) {
-                    lid[s] = __ffs(hm) - 1;
-                    hm &= hm - 1;
-                    ++cnt;
-                }
-            }
-            // first reads of the group's compressed rows: every lane's 16-byte pieces of all
-            // rows are loaded into registers before any is stored, so the rows' PCIe round
-            // trips overlap; rows that are not 16-byte aligned or longer than 1 KiB take a
-            // plain loop
-            {
-                constexpr int per16 = 16 / sizeof(U);
-                const int64_t nq = (a.first_words + per16 - 1) / per16;
-                uint4 stage[kRowsInFlight][2];
-                bool fast[kRowsInFlight];
-#pragma unroll
-                for (int s = 0; s < kRowsInFlight; ++s) {
-                    fast[s] = false;
-                    if (s < cnt) {
-                        const int64_t r = __shfl_sync(0xffffffffu, key, lid[s]);
-                        const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[s]);
-                        const U *row = a.comp + r * v;
-                        fast[s] = pk && ((((uintptr_t)row) & 15) == 0) && nq <= 64;
-                        if (fast[s]) {
-                            const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
-                            if (lane < nq) stage[s][0] = r4[lane];
-                            if (lane + 32 < nq) stage[s][1] = r4[lane + 32];
-                        } else if (pk) {
-                            issue_words<U>(slots + s * a.slot_words, row, 0, a.first_words);
-                        }
-                    }
-                }
-#pragma unroll
-                for (int s = 0; s < kRowsInFlight; ++s) {
-                    if (fast[s]) {
-                        uint4 *b4 = reinterpret_cast<uint4 *>(slots + s * a.slot_words);
-                        if (lane < nq) b4[lane] = stage[s][0];
-                        if (lane + 32 < nq) b4[lane + 32] = stage[s][1];
-                    }
-                }
-            }
-            __syncwarp();
-#pragma unroll
-            for (int s = 0; s < kRowsInFlight; ++s) {
-                if (s < cnt) {
-                    const int64_t r = __shfl_sync(0xffffffffu, key, lid[s]);
-                    const int64_t d = __shfl_sync(0xffffffffu, dst, lid[s]);
-                    const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[s]);
-                    const U *row = a.comp + r * v;
-                    U *orow = a.out + d * v;
-                    if (!pk) {
-                        warp_copy<U>(orow, row, v);
-                        continue;
-                    }
-                    U *buf = slots + s * a.slot_words;
-                    const int64_t end = row_words<U, NC>(buf, v, a.mw, a.t, lt);
-                    if (end >= v) {
-                        // a bitmap claiming a stream as long as the raw row cannot come from
-                        // this mask: report it and leave the output row alone
-                        if (lane == 0) atomicOr(a.status, kStatusCorruptRow);
-                        continue;
-                    }
-                    if (end > a.first_words) {  // longer than the hint: fetch the rest
-                        issue_words<U>(buf, row, a.first_words, end);
-                    }
-                    __syncwarp();
-                    // words past the stream read as zero (get_bits looks one word ahead;
-                    // the value there never reaches an output bit)
-                    if (lane < 2) buf[end + lane] = 0;
-                    __syncwarp();
-                    decode_row<U, NC>(buf, v, a.mw, a.t, lt, orow);
-                    __syncwarp();
-                }
-            }
-        }
+            head && !a.raw_only && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1);
+        fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head, packed,
+                           a.status);
     }
 }
 
@@ -437,7 +227,7 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     const size_t smem = slot_bytes * slots * (threads / 32);
     if ((int64_t)smem > maxs) {
         set_error("rows of %lld words do not fit the fetch kernel's shared-memory slot",
-                  (long long)a.v);
+                  (long long)a.s.v);
         return IBP_ERR_UNSUPPORTED;
     }
     a.slots = slots;
@@ -463,9 +253,9 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
 template <typename U>
 static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStream_t st) {
     if (a.nrows <= 0) return IBP_OK;
-    a.slot_words = (int64_t)align_up((size_t)a.v + 2, 16 / sizeof(U));
-    if (a.raw_only || a.v > 64) return launch_fetch_nc<U, 0>(a, nblks, nthreads, st);
-    if (a.v > 32) return launch_fetch_nc<U, 2>(a, nblks, nthreads, st);
+    a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, 16 / sizeof(U));
+    if (a.raw_only || a.s.v > 64) return launch_fetch_nc<U, 0>(a, nblks, nthreads, st);
+    if (a.s.v > 32) return launch_fetch_nc<U, 2>(a, nblks, nthreads, st);
     return launch_fetch_nc<U, 1>(a, nblks, nthreads, st);
 }
 
@@ -491,26 +281,18 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     if (impl != 2) IBP_RET(build_tables<U>(mask, bitval, v, t, st));
 
     FetchArgs<U> a{};
-    a.comp = comp;
-    a.n = n;
-    a.v = v;
-    a.mw = meta_bytes(v, wb) / wb;
-    a.t = t;
-    a.bitmask = bitmask;
+    a.s.comp = comp;
+    a.s.n = n;
+    a.s.v = v;
+    a.s.mw = meta_bytes(v, wb) / wb;
+    a.s.t = t;
+    a.s.bitmask = bitmask;
+    a.s.first_words = first_read_words(v, a.s.mw, wb, comp_len);
     a.nrows = nrows;
     a.raw_only = impl == 2;
     a.out = out;
     a.status = status;
     a.work = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 64);
-    // first read of a compressed row: the hint (average compressed words) plus one word,
-    // rounded up to whole 32-byte sectors; without a hint, the first 128 bytes
-    {
-        const int64_t sector = 32 / wb;
-        int64_t want = (comp_len > 0 && comp_len < v) ? (int64_t)comp_len + 1 : 128 / wb;
-        if (want < a.mw + 1) want = a.mw + 1;
-        want = (want + sector - 1) / sector * sector;
-        a.first_words = want < v ? want : v;
-    }
     if (!has_index) return launch_fetch<U>(a, nblks, nthreads, st);
 
     if (nidx > 0x7fffffffLL) {

@@ -1,0 +1,249 @@
+// ibp_fetch.cuh -- device code shared by the per-call fetch (ibp_decompress.cu) and the
+// batched multi-set fetch (ibp_batch.cu): row reads into shared-memory slots, the
+// per-column tables a lane keeps, the row decoder, and the processing of one chunk's
+// distinct rows with several first reads in flight per warp.
+#pragma once
+
+#include "ibp_codec.cuh"
+#include "ibp_common.cuh"
+
+namespace ibp200 {
+
+constexpr int kRowsInFlight = 4;  // first reads a warp keeps outstanding
+
+// One tensor set as the fetch kernels see it.
+template <typename U>
+struct RowSet {
+    const U *comp;          // fixed-stride compressed rows (device or pinned host)
+    int64_t n, v, mw;       // rows, words per row, bitmap words
+    int64_t first_words;    // words of the first read of a compressed row
+    ColTables<U> t;         // per-column tables (device)
+    const int32_t *bitmask; // compressed-row bits (device)
+};
+
+// Copy row words [w0, w1) into the same positions of a shared slot: 16-byte loads when the
+// row is 16-byte aligned (whole aligned blocks; a block straddling w0 rewrites words already
+// present with the same values), word loads otherwise.
+template <typename U>
+__device__ __forceinline__ void issue_words(U *__restrict__ slot, const U *__restrict__ row,
+                                            int64_t w0, int64_t w1) {
+    const int lane = threadIdx.x & 31;
+    if ((((uintptr_t)row) & 15) == 0) {
+        constexpr int per16 = 16 / sizeof(U);
+        const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
+        uint4 *b4 = reinterpret_cast<uint4 *>(slot);
+        for (int64_t q = w0 / per16 + lane; q < (w1 + per16 - 1) / per16; q += 32) b4[q] = r4[q];
+    } else {
+        for (int64_t w = w0 + lane; w < w1; w += 32) slot[w] = row[w];
+    }
+}
+
+// ------------------------------------------------------------------ column tables
+// Tables of the columns j = lane + 32*c, c < NC, held in registers (NC = 1 or 2), or read
+// through L1 from the workspace copy (NC = 0, any row length).
+template <typename U, int NC>
+struct LaneTables {
+    static constexpr int LW = LogW<U>::value;
+    U m[NC > 0 ? NC : 1], bv[NC > 0 ? NC : 1], mv[NC > 0 ? NC : 1][LW];
+    int nb[NC > 0 ? NC : 1];
+
+    __device__ __forceinline__ void load(const ColTables<U> &t, int64_t v) {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int64_t j = lane + 32 * c;
+            const bool in = j < v;
+            m[c] = in ? t.mask[j] : (U)0;
+            bv[c] = in ? t.bitval[j] : (U)0;
+            nb[c] = in ? (int)t.nb[j] : 0;
+#pragma unroll
+            for (int i = 0; i < LW; ++i) mv[c][i] = in ? t.mv[i * v + j] : (U)0;
+        }
+    }
+};
+
+template <typename U>
+__device__ __forceinline__ U scatter_regs(U y, U sel, const U *mv) {
+    constexpr int LW = LogW<U>::value;
+#pragma unroll
+    for (int i = LW - 1; i >= 0; --i) {
+        const U t = (U)(y << (1 << i));
+        y = (U)((y & ~mv[i]) | (t & mv[i]));
+    }
+    return (U)(y & sel);
+}
+
+// Decode one compressed row from its shared-memory slot (bitmap at word 0, stream at word
+// mw, zero words after the stream) into the output row.
+template <typename U, int NC>
+__device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v, int64_t mw,
+                                           const ColTables<U> &t, const LaneTables<U, NC> &lt,
+                                           U *__restrict__ orow) {
+    constexpr int W = 8 * sizeof(U);
+    const int lane = threadIdx.x & 31;
+    const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
+    const U *stream = buf + mw;
+    int64_t base = 0;
+    auto chunk = [&](int64_t c0, U m, U bv, int nbits, const U *mv, int stride) {
+        const int64_t j = c0 + lane;
+        const bool in = j < v;
+        const bool cj = in && ((units[j >> 5] >> (j & 31)) & 1u);
+        const int L = in ? (cj ? nbits : W) : 0;
+        int incl = L;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (in) {
+            const U y = get_bits<U>(stream, base + incl - L, L);
+            U x = y;
+            if (cj) {
+                if (stride == 0)
+                    x = (U)(bv | scatter_regs<U>(y, (U)~m, mv));
+                else
+                    x = (U)(bv | scatter_bits<U>(y, (U)~m, mv, stride));
+            }
+            orow[j] = x;
+        }
+        base += __shfl_sync(0xffffffffu, incl, 31);
+    };
+    if constexpr (NC > 0) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            if (32 * c < v) chunk(32 * c, lt.m[c], lt.bv[c], lt.nb[c], lt.mv[c], 0);
+    } else {
+        for (int64_t c0 = 0; c0 < v; c0 += 32) {
+            const int64_t j = c0 + lane;
+            const bool in = j < v;
+            chunk(c0, in ? __ldg(&t.mask[j]) : (U)0, in ? __ldg(&t.bitval[j]) : (U)0,
+                  in ? (int)__ldg(&t.nb[j]) : 0, t.mv + (in ? j : 0), (int)v);
+        }
+    }
+}
+
+// Exact compressed words of the row whose bitmap is in the slot (bitmap + stream).
+template <typename U, int NC>
+__device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t v, int64_t mw,
+                                             const ColTables<U> &t,
+                                             const LaneTables<U, NC> &lt) {
+    constexpr int W = 8 * sizeof(U);
+    const int lane = threadIdx.x & 31;
+    const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
+    uint32_t bits = 0;
+    if constexpr (NC > 0) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int64_t j = lane + 32 * c;
+            if (j < v) bits += ((units[j >> 5] >> (j & 31)) & 1u) ? (uint32_t)lt.nb[c] : (uint32_t)W;
+        }
+    } else {
+        for (int64_t j = lane; j < v; j += 32)
+            bits += ((units[j >> 5] >> (j & 31)) & 1u) ? (uint32_t)__ldg(&t.nb[j]) : (uint32_t)W;
+    }
+    bits = __reduce_add_sync(0xffffffffu, bits);
+    return mw + (bits + W - 1) / W;
+}
+
+
+// Fetch and decode (or copy, when not packed) the rows of the lanes whose `head` is set:
+// groups of up to `nslots` rows have their first reads loaded into registers together (16-
+// byte loads, all rows before any store), so their PCIe or HBM round trips overlap; rows
+// that are not 16-byte aligned or whose first read exceeds 1 KiB take a plain loop.
+// `orow` is each lane's output row.
+template <typename U, int NC>
+__device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables<U, NC> &lt,
+                                            U *__restrict__ slots, int nslots,
+                                            int64_t slot_words, int64_t key, U *orow,
+                                            bool head, bool packed, int32_t *status) {
+    const int lane = threadIdx.x & 31;
+    const int64_t v = s.v;
+    unsigned hm = __ballot_sync(0xffffffffu, head);
+    while (hm) {
+        int lid[kRowsInFlight];
+        int cnt = 0;
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            lid[q] = 0;
+            if (q < nslots && hm) {
+                lid[q] = __ffs(hm) - 1;
+                hm &= hm - 1;
+                ++cnt;
+            }
+        }
+        {
+            constexpr int per16 = 16 / sizeof(U);
+            const int64_t nq = (s.first_words + per16 - 1) / per16;
+            uint4 stage[kRowsInFlight][2];
+            bool fast[kRowsInFlight];
+#pragma unroll
+            for (int q = 0; q < kRowsInFlight; ++q) {
+                fast[q] = false;
+                if (q < cnt) {
+                    const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+                    const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[q]);
+                    const U *row = s.comp + r * v;
+                    fast[q] = pk && ((((uintptr_t)row) & 15) == 0) && nq <= 64;
+                    if (fast[q]) {
+                        const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
+                        if (lane < nq) stage[q][0] = r4[lane];
+                        if (lane + 32 < nq) stage[q][1] = r4[lane + 32];
+                    } else if (pk) {
+                        issue_words<U>(slots + q * slot_words, row, 0, s.first_words);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kRowsInFlight; ++q) {
+                if (fast[q]) {
+                    uint4 *b4 = reinterpret_cast<uint4 *>(slots + q * slot_words);
+                    if (lane < nq) b4[lane] = stage[q][0];
+                    if (lane + 32 < nq) b4[lane + 32] = stage[q][1];
+                }
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            if (q < cnt) {
+                const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+                U *o = reinterpret_cast<U *>(
+                    __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
+                const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[q]);
+                const U *row = s.comp + r * v;
+                if (!pk) {
+                    warp_copy<U>(o, row, v);
+                    continue;
+                }
+                U *buf = slots + q * slot_words;
+                const int64_t end = row_words<U, NC>(buf, v, s.mw, s.t, lt);
+                if (end >= v) {
+                    // a bitmap claiming a stream as long as the raw row cannot come from this
+                    // mask: report it and leave the output row alone
+                    if (lane == 0) atomicOr(status, kStatusCorruptRow);
+                    continue;
+                }
+                if (end > s.first_words) issue_words<U>(buf, row, s.first_words, end);
+                __syncwarp();
+                // words past the stream read as zero (get_bits looks one word ahead; the
+                // value there never reaches an output bit)
+                if (lane < 2) buf[end + lane] = 0;
+                __syncwarp();
+                decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
+                __syncwarp();
+            }
+        }
+    }
+}
+
+// Words of the first read of a compressed row: the caller's average-length hint plus one
+// word, rounded up to whole 32-byte sectors; without a hint, the first 128 bytes.
+inline int64_t first_read_words(int64_t v, int64_t mw, int wb, int comp_len) {
+    const int64_t sector = 32 / wb;
+    int64_t want = (comp_len > 0 && comp_len < v) ? (int64_t)comp_len + 1 : 128 / wb;
+    if (want < mw + 1) want = mw + 1;
+    want = (want + sector - 1) / sector * sector;
+    return want < v ? want : v;
+}
+
+}  // namespace ibp200
