@@ -43,6 +43,11 @@ def parse():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--config", default="graph_features",
+                    choices=["graph_features", "embedding_tables", "decoder_layer",
+                             "served_mix"])
+    ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
+    ap.add_argument("--requests", type=int, default=300)
     return ap.parse_args()
 
 
@@ -273,8 +278,319 @@ def reference_gpu(torch, comp, m, b, bm, comp_len, batches_dev, steps):
                     "nblks=2*SMs) on the same compressed rows and index arrays"}, out
 
 
+def run_batched(args):
+    """One batched, graph-replayed launch per step over many tensor sets, against one
+    decompress_fetch call per set (the reference's calling pattern).
+
+    embedding_tables: 26 tables of 64 fp32 (int64 [rows, 32]), rows log-uniform in
+      [1e4, 4e6], per-table mask preprocess(0.9); a step fetches 2048 Zipf(1.05) rows of every
+      table.  decoder_layer: the 9 tensor sets of one 4096-hidden decoder layer (fp16 weights
+      and one layer of KV cache, int64 rows of 512 words), sweep masks; a step fetches all
+      115,200 rows."""
+    import torch
+    torch.cuda.set_device(0)
+    import invariantbitpacking_b200 as ibp
+    from invariantbitpacking_b200 import _capi, synthetic
+    from invariantbitpacking_b200.batch import BatchFetcher, SetRegistry
+    lib = _capi.lib
+    t0 = time.perf_counter()
+    if args.config == "embedding_tables":
+        arrays = synthetic.embedding_tables()
+        thr = 0.9
+    else:
+        arrays = list(synthetic.decoder_layer().values())
+        thr = None
+    gen_s = time.perf_counter() - t0
+    sets, sizes = [], []
+    t0 = time.perf_counter()
+    for a in arrays:
+        x = torch.from_numpy(a).pin_memory()
+        m, b = ibp.preprocess(x, thr)
+        sizes.append(ibp.get_compress_size(x, m, b))
+        bm = ibp.compress_inplace(x, m, b)
+        sets.append((x, m, b, bm, ibp.get_single_compress_len(x, m, b)))
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t0
+    sizes = [sz.numpy().copy() for sz in sizes]
+    km = None
+    if args.config == "embedding_tables":
+        t0 = time.perf_counter()
+        for a in arrays:
+            ibp.preprocess_kmeans(torch.from_numpy(a).pin_memory(), 16, 0.9)
+        km = round(time.perf_counter() - t0, 3)
+    nsets = len(sets)
+    v = [s[0].shape[1] for s in sets]
+    variants = []
+    if args.config == "embedding_tables":
+        zs = [synthetic.Zipf(a.shape[0], 1.05, seed=100 + i) for i, a in enumerate(arrays)]
+        for _ in range(6):
+            variants.append([(i, torch.from_numpy(zs[i].sample(2048)).cuda(), 0, 2048)
+                             for i in range(nsets)])
+    else:
+        variants.append([(i, None, 0, sets[i][0].shape[0]) for i in range(nsets)])
+    outs = [[torch.empty((r[3], v[r[0]]), dtype=torch.int64, device="cuda") for r in reqs]
+            for reqs in variants]
+    step_bytes = [sum(r[3] * v[r[0]] * 8 for r in reqs) for reqs in variants]
+    comp_bytes = []
+    for reqs in variants:
+        cb = 0
+        for sid, idx, first, count in reqs:
+            sz = sizes[sid]
+            cb += int(sz[idx.cpu().numpy()].sum()) if idx is not None else int(sz[first:first + count].sum())
+        comp_bytes.append(cb)
+    reg = SetRegistry(sets)
+    bf = BatchFetcher(reg, max_requests=nsets)
+    # correctness of every variant before timing
+    for reqs, o in zip(variants, outs):
+        bf.fetch(reqs, o)
+        torch.cuda.synchronize()
+        for (sid, idx, first, count), oo in zip(reqs, o):
+            want = arrays[sid][idx.cpu().numpy()] if idx is not None else arrays[sid][first:first + count]
+            assert np.array_equal(oo.cpu().numpy(), want), "batched fetch mismatch"
+    shape = bf.autotune(variants[0], outs[0])
+    bf.capture()
+    for k in range(args.warmup):
+        bf.fetch(variants[k % len(variants)], outs[k % len(variants)])
+    torch.cuda.synchronize()
+    # each step replays the captured graph: the request-table copy and one batch kernel
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with Clocks(torch.cuda.current_device()) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tot = cb_tot = 0
+        for k in range(args.steps):
+            j = k % len(variants)
+            evs[k][0].record()
+            bf.fetch(variants[j], outs[j])
+            evs[k][1].record()
+            tot += step_bytes[j]
+            cb_tot += comp_bytes[j]
+        e1.record()
+        e1.synchronize()
+    kms = [a.elapsed_time(b) for a, b in evs]
+    nk = len(kms)
+    launches = args.steps  # one engine kernel per graph replay
+    ms = e0.elapsed_time(e1)
+    value = tot / ms / 1e6
+    # per-call: one decompress_fetch per set, the reference's calling pattern
+    for k in range(args.warmup):
+        reqs = variants[k % len(variants)]
+        for (sid, idx, first, count), oo in zip(reqs, outs[k % len(variants)]):
+            x, m, b, bm, cl = sets[sid]
+            ibp.decompress_fetch(x, m, b, bm, torch.device("cuda"), cl, idx, output_tensor=oo)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    ptot = 0
+    for k in range(args.steps):
+        j = k % len(variants)
+        for (sid, idx, first, count), oo in zip(variants[j], outs[j]):
+            x, m, b, bm, cl = sets[sid]
+            ibp.decompress_fetch(x, m, b, bm, torch.device("cuda"), cl, idx, output_tensor=oo)
+        ptot += step_bytes[j]
+    p1.record()
+    p1.synchronize()
+    pms = p0.elapsed_time(p1)
+    pcie = measured_pcie_h2d(torch)
+    kavg = sum(kms) / max(len(kms), 1)
+    ach = (sum(comp_bytes[k % len(variants)] for k in range(nk)) / sum(kms) / 1e6) if kms else None
+    name = {"embedding_tables": "26 embedding tables x 2048 Zipf(1.05) rows",
+            "decoder_layer": "one decoder layer: 9 tensor sets, 115,200 rows of 4 KiB"}[args.config]
+    line = {
+        "metric": f"batched decompress_fetch delivered GB/s ({name}, host-resident)",
+        "value": round(value, 3), "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic",
+        "config": {"workload": args.config, "sets": nsets,
+                   "rows_per_set": [int(s[0].shape[0]) for s in sets],
+                   "delivered_bytes_per_step": step_bytes[0],
+                   "compressed_fraction": round(sum(int(z.sum()) for z in sizes) /
+                                                sum(a.nbytes for a in arrays), 4),
+                   "launch_shape": shape, "graph": True,
+                   "setup_s": {"generate": round(gen_s, 2), "preprocess_compress": round(prep_s, 2),
+                               "preprocess_kmeans_all_tables": km}},
+        "per_call": {"value": round(ptot / pms / 1e6, 3), "unit": "GB/s",
+                     "ms_per_step": round(pms / args.steps, 4),
+                     "what": f"{nsets} ibp.decompress_fetch calls per step, one per set"},
+        "roofline": {"bound": "pcie", "achieved": None if ach is None else round(ach, 3),
+                     "peak": round(pcie, 3), "unit": "GB/s",
+                     "frac": None if ach is None else round(ach / pcie, 4), "traffic": None,
+                     "what": "batch_fetch_kernel: compressed bytes of the fetched rows / CUDA-"
+                             "event time of each graph replay (a 4 KB table copy + the kernel)",
+                     "kernel_ms_per_launch": round(kavg, 4),
+                     "peak_source": "pinned host->device copy measured in this run"},
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def served_sets(torch, ibp):
+    """8 host-pinned sets from the plain/graph/embedding generators, rows re-shaped to
+    V in {64, 128, 256, 512} int64 words, ~384 MB each."""
+    from invariantbitpacking_b200 import synthetic
+    plan = [("graph", 64), ("plain", 128), ("embed", 256), ("graph", 512),
+            ("plain", 64), ("embed", 128), ("graph", 256), ("plain", 512)]
+    target = 384 << 20
+    srcs, sets = [], []
+    for i, (gen, v) in enumerate(plan):
+        rows = target // (v * 8)
+        if gen == "graph":
+            f = synthetic.graph_features(n=rows * v // 64, seed=40 + i).view(np.float32)
+        elif gen == "plain":
+            f = synthetic.plain_small(n=rows * v // 128, seed=40 + i)[0].view(np.float32)
+        else:
+            f = np.concatenate([t.view(np.float32).reshape(-1) for t in synthetic.embedding_tables(
+                num_tables=(2 * v + 63) // 64, seed=40 + i, min_rows=rows, max_rows=rows + 1)])
+        d = np.ascontiguousarray(f.reshape(-1)[:rows * v * 2]).view(np.int64).reshape(rows, v)
+        x = torch.from_numpy(d).pin_memory()
+        m, b = ibp.preprocess(x, None)
+        bm = ibp.compress_inplace(x, m, b)
+        srcs.append(d)
+        sets.append((x, m, b, bm, ibp.get_single_compress_len(x, m, b)))
+    return srcs, sets
+
+
+def run_served(args):
+    """Poisson request streams over 8 sets; requests of log-uniform [256, 262144] rows with
+    uniform row numbers; the continuous-batching server (40 GB output arena) against one
+    plain decompress_fetch per request in arrival order.  Latency = completion time minus
+    scheduled arrival time."""
+    import threading
+    import torch
+    torch.cuda.set_device(0)
+    import invariantbitpacking_b200 as ibp
+    from invariantbitpacking_b200.batch import SetRegistry
+    from invariantbitpacking_b200.serve import Server
+    t0 = time.perf_counter()
+    srcs, sets = served_sets(torch, ibp)
+    setup_s = time.perf_counter() - t0
+    reg = SetRegistry(sets)
+    srv = Server(reg, arena_bytes=40 << 30, index_capacity=1 << 26, max_batch=256,
+                 max_inflight=2)
+    rates = [float(r) for r in args.rates.split(",")]
+    nreq = args.requests
+    rng = np.random.default_rng(7)
+    results = []
+    checked = 0
+    for rate in rates:
+        gaps = rng.exponential(1.0 / rate, nreq)
+        arrive = np.cumsum(gaps)
+        sids = rng.integers(0, len(sets), nreq)
+        counts = np.exp(rng.uniform(np.log(256), np.log(262144), nreq)).astype(np.int64)
+        rows = [rng.integers(0, srcs[s].shape[0], c).astype(np.int64) for s, c in zip(sids, counts)]
+        total_bytes = int(sum(c * srcs[s].shape[1] * 8 for s, c in zip(sids, counts)))
+
+        # ---- served: a client thread submits on schedule, the main thread waits/releases
+        ids = [None] * nreq
+        base = time.monotonic() + 0.05
+
+        def client():
+            for j in range(nreq):
+                t = base + arrive[j]
+                while time.monotonic() < t:
+                    pass
+                while True:
+                    try:
+                        ids[j] = srv.submit(int(sids[j]), rows[j])
+                        break
+                    except RuntimeError:
+                        time.sleep(0.0002)
+
+        th = threading.Thread(target=client)
+        th.start()
+        lat = []
+        t_last = 0.0
+        for j in range(nreq):
+            while ids[j] is None:
+                time.sleep(0.0001)
+            out, tm = srv.wait(ids[j], 600000)
+            if checked < 24 and j % 13 == 0:
+                assert np.array_equal(out.cpu().numpy(), srcs[sids[j]][rows[j]]), "served mismatch"
+                checked += 1
+            srv.release(ids[j])
+            lat.append(tm[2] / 1e6 - (base + arrive[j]))
+            t_last = max(t_last, tm[2] / 1e6)
+        th.join()
+        served = {"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                  "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                  "GBps": round(total_bytes / (t_last - base) / 1e9, 3)}
+
+        # ---- per request: one plain decompress_fetch per request, in arrival order
+        rows_pin = [torch.from_numpy(r).pin_memory() for r in rows]
+        evs = [None] * nreq
+        done_t = [0.0] * nreq
+        base2 = time.monotonic() + 0.05
+
+        def reaper():
+            for j in range(nreq):
+                while evs[j] is None:
+                    time.sleep(0.00005)
+                evs[j].synchronize()
+                done_t[j] = time.monotonic()
+
+        rt = threading.Thread(target=reaper)
+        rt.start()
+        outs = [None] * nreq
+        for j in range(nreq):
+            t = base2 + arrive[j]
+            while time.monotonic() < t:
+                pass
+            x, m, b, bm, cl = sets[sids[j]]
+            idx = rows_pin[j].to("cuda", non_blocking=True)
+            outs[j] = ibp.decompress_fetch(x, m, b, bm, torch.device("cuda"), cl, idx)
+            ev = torch.cuda.Event()
+            ev.record()
+            evs[j] = ev
+            if j >= 2:
+                outs[j - 2] = None  # let the caching allocator reuse finished outputs
+        rt.join()
+        lat2 = [done_t[j] - (base2 + arrive[j]) for j in range(nreq)]
+        plain = {"p50_ms": round(float(np.percentile(lat2, 50)) * 1e3, 3),
+                 "p99_ms": round(float(np.percentile(lat2, 99)) * 1e3, 3),
+                 "GBps": round(total_bytes / (max(done_t) - base2) / 1e9, 3)}
+        del outs
+        torch.cuda.empty_cache()
+        results.append({"rate_per_s": rate, "requests": nreq,
+                        "output_GB": round(total_bytes / 1e9, 2), "served": served,
+                        "per_request": plain})
+    st = srv.stats()
+    srv.close()
+    head = results[0]
+    line = {
+        "metric": "served mix: continuous-batching server vs per-request decompress_fetch "
+                  "(p50/p99 latency, delivered GB/s)",
+        "value": head["served"]["GBps"], "unit": "GB/s", "n_gpus": 1, "steps": nreq,
+        "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "served_mix: 8 pinned sets (~384 MB each), V in {64,128,256,512}, "
+                               "Poisson arrivals, log-uniform [256, 262144] rows per request",
+                   "arena_GB": 40, "max_batch": 256, "max_inflight": 2,
+                   "setup_s": round(setup_s, 1), "batches": st["batches"],
+                   "bit_exact_checked_requests": checked},
+        "rates": results,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.config == "served_mix":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the served configuration "
+                              "compares against per-request fetches in the same line"}))
+            return
+        run_served(args)
+        return
+    if args.config != "graph_features":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched configurations "
+                              "are measured against per-call fetches in the same line"}))
+            return
+        run_batched(args)
+        return
     if args.impl == "reference":
         ws = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

@@ -218,6 +218,33 @@ ibp_status ibp_batch_autotune(const void *registry, const ibp_request *requests,
                               void *workspace, size_t workspace_bytes, int32_t *chosen,
                               ibp_stream_t stream);
 
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference (its callers issue one decompress_fetch per lookup).  A
+ * continuous-batching server over a registry: clients submit requests from any thread; a
+ * scheduler thread admits them in arrival order whenever their output fits the caller's
+ * device arena, packs all admitted requests into one batched launch, and keeps up to
+ * max_inflight launches on the GPU, so requests arriving meanwhile join the next launch.
+ * Buffers (index staging rings of index_capacity entries, request tables, a stream) are
+ * allocated at creation only.  Timestamps are host steady-clock microseconds. */
+typedef struct ibp_server ibp_server;
+ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int32_t nsets,
+                             int word_bytes, void *out_arena, size_t arena_bytes,
+                             int64_t index_capacity, int32_t max_batch, int32_t max_inflight,
+                             ibp_server **out);
+/* rows == NULL: rows first .. first+count-1; else `count` host row numbers (copied before
+ * returning).  IBP_ERR_WORKSPACE: index staging full (retry) or output larger than the arena. */
+ibp_status ibp_server_submit(ibp_server *srv, int32_t set, const int64_t *rows, int64_t first,
+                             int64_t count, int64_t *id);
+/* Wait for a request (timeout_ms < 0: forever); *out = its output rows in the arena,
+ * times[0..2] = submitted, admitted, done.  IBP_ERR_UNSUPPORTED on timeout. */
+ibp_status ibp_server_wait(ibp_server *srv, int64_t id, int32_t timeout_ms, void **out,
+                           double *times);
+/* Give a finished request's output rows back to the arena. */
+ibp_status ibp_server_release(ibp_server *srv, int64_t id);
+/* stats[0..3] = batches launched, rows done, output bytes done, requests pending. */
+ibp_status ibp_server_stats(ibp_server *srv, int64_t *stats);
+ibp_status ibp_server_destroy(ibp_server *srv);
+
 /* ---------------------------------------------------------------- decompress_fetch, no allocation
  * No counterpart in the reference.  For callers that cannot allocate device memory at all
  * (a host framework that owns every device byte and offers no allocation hook, an allocator

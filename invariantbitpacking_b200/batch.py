@@ -50,6 +50,7 @@ class SetRegistry:
             d.mask, d.bitval, d.bitmask = mask.data_ptr(), bitval.data_ptr(), bitmask.data_ptr()
             d.comp_len = comp_len
             self.sets.append((comp, mask, bitval, bitmask))
+        self.descs = descs
         self.word_bytes = wb
         self.dtype = sets[0][0].dtype
         self.vec_sizes = [s[0].shape[1] for s in self.sets]

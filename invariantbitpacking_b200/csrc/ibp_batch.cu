@@ -7,8 +7,6 @@
 //
 // The reference fetches one set per decompress_fetch call (src/decompress.cu:10-156); its
 // embedding-bag and decoder-layer callers issue one call per table or tensor.
-#include <cub/block/block_scan.cuh>
-
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -20,8 +18,6 @@
 #include "ibp_internal.cuh"
 
 namespace ibp200 {
-
-constexpr int kBatchScanThreads = 256;
 
 // Device layout of a registry: header, then nsets RowSet<U>, then every set's tables.
 struct RegistryHeader {
@@ -55,33 +51,50 @@ struct BatchArgs {
     int slots;
 };
 
+// Shared-memory head of the batch kernel: max_req + 1 unit prefixes and up to 256
+// per-thread partial sums.
+__host__ __device__ inline size_t batch_head_bytes(int max_req) {
+    return align_up(sizeof(int64_t) * ((size_t)max_req + 1 + 256), 16);
+}
+
 // Units of 32 rows: request r owns units [prefix[r], prefix[r+1]).
 template <typename U, int NC>
 __global__ void __launch_bounds__(256) batch_fetch_kernel(BatchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     int64_t *prefix = reinterpret_cast<int64_t *>(smem);
-    U *slots = reinterpret_cast<U *>(smem + align_up(sizeof(int64_t) * (a.max_req + 1), 16)) +
+    U *slots = reinterpret_cast<U *>(smem + batch_head_bytes(a.max_req)) +
                (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
     const int nreq = min(max(*a.nreq, 0), a.max_req);
-    // block-wide exclusive scan of the requests' unit counts
+    // exclusive scan of the requests' unit counts, for any block size: each thread sums a
+    // contiguous segment of requests, thread 0 scans the per-thread sums, each thread then
+    // writes its segment's prefixes
     {
-        const int per = (nreq + blockDim.x - 1) / blockDim.x;
-        const int r0 = threadIdx.x * per;
+        int64_t *part = prefix + a.max_req + 1;  // blockDim.x partial sums
+        const int per = (nreq + (int)blockDim.x - 1) / (int)blockDim.x;
+        const int r0 = (int)threadIdx.x * per;
         int64_t sum = 0;
         for (int r = r0; r < r0 + per && r < nreq; ++r) {
             const int64_t cnt = a.reqs[r].count;
             sum += cnt > 0 ? (cnt + 31) / 32 : 0;
         }
-        typedef cub::BlockScan<int64_t, 256> Scan;
-        __shared__ typename Scan::TempStorage tmp;
-        int64_t excl = 0, total = 0;
-        Scan(tmp).ExclusiveSum(sum, excl, total);
+        part[threadIdx.x] = sum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t run = 0;
+            for (int t = 0; t < (int)blockDim.x; ++t) {
+                const int64_t x = part[t];
+                part[t] = run;
+                run += x;
+            }
+            prefix[nreq] = run;
+        }
+        __syncthreads();
+        int64_t excl = part[threadIdx.x];
         for (int r = r0; r < r0 + per && r < nreq; ++r) {
             prefix[r] = excl;
             const int64_t cnt = a.reqs[r].count;
             excl += cnt > 0 ? (cnt + 31) / 32 : 0;
         }
-        if (threadIdx.x == 0) prefix[nreq] = total;
         __syncthreads();
     }
     const int lane = threadIdx.x & 31;
@@ -215,7 +228,7 @@ static std::map<ShapeKey, Shape> g_shapes;
 template <typename U, int NC>
 static ibp_status launch_batch_nc(BatchArgs<U> a, int64_t max_v, Shape sh, cudaStream_t st) {
     const size_t slot_bytes = (size_t)a.slot_words * sizeof(U);
-    const size_t head = align_up(sizeof(int64_t) * (a.max_req + 1), 16);
+    const size_t head = batch_head_bytes(a.max_req);
     int threads = sh.threads;
     int slots = std::max(1, std::min(sh.slots, kRowsInFlight));
     const int maxs = device_max_smem_optin();

@@ -1,0 +1,455 @@
+// ibp_server.cu -- a continuous-batching decompress_fetch server.
+//
+// Clients submit requests (registered set, host row list, count) from any thread; a
+// scheduler thread admits them in arrival order as output memory frees up, packs every
+// admitted request into one batched launch (ibp_batch_fetch over the set registry), and
+// keeps up to `max_inflight` batches on the GPU at once, so requests that arrive while
+// others run join the next launch instead of waiting for the queue to drain.  Completion is
+// stamped by a host callback queued behind each batch (no polling).
+//
+// Memory (all reserved at creation, nothing allocated per request):
+//   * output arena: the caller's device buffer; a first-fit free list with coalescing hands
+//     each request its rows, which stay valid until the client releases the request;
+//   * index staging: a pinned host ring and a device ring of the same size; submit copies the
+//     client's row list into the host ring, the batch copies its span to the device ring;
+//   * request tables: one pinned + one device table per in-flight batch.
+//
+// The reference has no serving layer: its callers (ColossalAI embedding bags, FlexGen
+// layers, DGL samplers) call decompress_fetch once per lookup.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "ibp_internal.cuh"
+
+namespace ibp200 {
+
+using Clock = std::chrono::steady_clock;
+
+static double now_us() {
+    return std::chrono::duration<double, std::micro>(Clock::now().time_since_epoch()).count();
+}
+
+struct SrvRequest {
+    int64_t id;
+    int32_t set;
+    int64_t count;
+    int64_t first;
+    bool has_index;
+    int64_t idx_off;    // element offset of the row list in the index rings (-1: none)
+    int64_t ring_end;   // ring position (monotonic) just past this request's row list
+    int64_t out_off;    // byte offset in the output arena (-1: not admitted yet)
+    int64_t out_bytes;
+    double t_submit, t_admit, t_done;
+    bool done = false;
+    bool released = false;
+};
+
+struct Batch {
+    std::vector<int64_t> ids;
+    int64_t idx_begin = 0, idx_end = 0;  // index-ring span [begin, end), monotonic positions
+    int table = 0;
+    bool complete = false;
+};
+
+struct Server {
+    const void *registry = nullptr;
+    std::vector<int64_t> set_v;      // words per row of each set
+    std::vector<int64_t> set_n;
+    int word_bytes = 8;
+    int max_batch = 0, max_inflight = 2;
+    char *arena = nullptr;
+    size_t arena_bytes = 0;
+    std::map<int64_t, int64_t> free_list;  // offset -> bytes
+    int64_t *idx_host = nullptr, *idx_dev = nullptr;
+    // ring positions are monotonic counters (physical slot = position % idx_cap):
+    // [tail, head) is reserved, [tail, launched) already copied to the device
+    int64_t idx_cap = 0, idx_head = 0, idx_tail = 0, idx_launched = 0;
+    std::vector<char *> tbl_host, tbl_dev;
+    std::vector<bool> tbl_busy;
+    void *ws = nullptr;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+
+    std::mutex mu;
+    std::condition_variable cv;       // scheduler wake-ups
+    std::condition_variable done_cv;  // client waits
+    std::deque<int64_t> pending;
+    std::map<int64_t, SrvRequest> reqs;
+    std::deque<Batch *> inflight;
+    int64_t next_id = 1;
+    bool stop = false;
+    std::thread thr;
+    std::string err;
+    // stats
+    int64_t batches = 0, rows_done = 0, bytes_done = 0;
+};
+
+static constexpr int kTableHeader = 64;
+
+// ---------------------------------------------------------------- arena allocation
+static int64_t arena_alloc(Server *s, int64_t bytes) {
+    bytes = (int64_t)align_up((size_t)bytes, 256);
+    for (auto it = s->free_list.begin(); it != s->free_list.end(); ++it) {
+        if (it->second >= bytes) {
+            const int64_t off = it->first, left = it->second - bytes;
+            s->free_list.erase(it);
+            if (left > 0) s->free_list[off + bytes] = left;
+            return off;
+        }
+    }
+    return -1;
+}
+
+static void arena_free(Server *s, int64_t off, int64_t bytes) {
+    bytes = (int64_t)align_up((size_t)bytes, 256);
+    auto it = s->free_list.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != s->free_list.end() && it->first + it->second == nx->first) {
+        it->second += nx->second;
+        s->free_list.erase(nx);
+    }
+    if (it != s->free_list.begin()) {
+        auto pv = std::prev(it);
+        if (pv->first + pv->second == it->first) {
+            pv->second += it->second;
+            s->free_list.erase(it);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- index ring
+static int64_t ring_used(const Server *s) { return s->idx_head - s->idx_tail; }
+
+// Reserve n contiguous elements; a reservation never wraps (the ring skips to 0 instead).
+static int64_t ring_reserve(Server *s, int64_t n) {
+    if (n > s->idx_cap) return -1;
+    int64_t pos = s->idx_head % s->idx_cap;
+    int64_t skip = 0;
+    if (pos + n > s->idx_cap) {
+        skip = s->idx_cap - pos;
+        pos = 0;
+    }
+    if (ring_used(s) + skip + n > s->idx_cap) return -1;
+    s->idx_head += skip + n;
+    return pos;
+}
+
+// ---------------------------------------------------------------- completion callback
+struct DoneCtx {
+    Server *s;
+    Batch *b;
+};
+
+static void CUDART_CB batch_done(void *p) {
+    DoneCtx *c = static_cast<DoneCtx *>(p);
+    const double t = now_us();
+    {
+        std::lock_guard<std::mutex> g(c->s->mu);
+        for (int64_t id : c->b->ids) {
+            auto it = c->s->reqs.find(id);
+            if (it != c->s->reqs.end()) {
+                it->second.t_done = t;
+                it->second.done = true;
+                c->s->rows_done += it->second.count;
+                c->s->bytes_done += it->second.out_bytes;
+            }
+        }
+        c->b->complete = true;
+    }
+    c->s->cv.notify_all();
+    c->s->done_cv.notify_all();
+    delete c;
+}
+
+// ---------------------------------------------------------------- scheduler
+static void retire(Server *s) {
+    // completed batches in launch order: free their index span and table
+    while (!s->inflight.empty() && s->inflight.front()->complete) {
+        Batch *b = s->inflight.front();
+        s->inflight.pop_front();
+        s->idx_tail = b->idx_end;
+        s->tbl_busy[b->table] = false;
+        delete b;
+    }
+}
+
+static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
+    int table = -1;
+    for (int t = 0; t < (int)s->tbl_busy.size(); ++t)
+        if (!s->tbl_busy[t]) {
+            table = t;
+            break;
+        }
+    if (table < 0 || s->pending.empty()) return false;
+    Batch *b = new Batch();
+    b->table = table;
+    b->idx_begin = s->idx_launched;
+    b->idx_end = s->idx_launched;
+    std::vector<ibp_request> recs;
+    // admit in arrival order while the output fits (head-of-line: an oversized request
+    // waits for memory, later ones wait behind it to keep arrival order)
+    while (!s->pending.empty() && (int)recs.size() < s->max_batch) {
+        SrvRequest &r = s->reqs[s->pending.front()];
+        const int64_t off = arena_alloc(s, r.out_bytes);
+        if (off < 0) break;
+        r.out_off = off;
+        r.t_admit = now_us();
+        ibp_request q{};
+        q.set = r.set;
+        q.index = r.has_index ? s->idx_dev + r.idx_off : nullptr;
+        q.first = r.first;
+        q.count = r.count;
+        q.out = s->arena + off;
+        recs.push_back(q);
+        b->ids.push_back(r.id);
+        b->idx_end = std::max(b->idx_end, r.ring_end);
+        s->pending.pop_front();
+    }
+    if (recs.empty()) {
+        delete b;
+        return false;
+    }
+    s->idx_launched = b->idx_end;
+    s->tbl_busy[table] = true;
+    char *th = s->tbl_host[table], *td = s->tbl_dev[table];
+    *reinterpret_cast<int32_t *>(th) = (int32_t)recs.size();
+    std::memcpy(th + kTableHeader, recs.data(), sizeof(ibp_request) * recs.size());
+    s->inflight.push_back(b);
+    s->batches++;
+    // the GPU work needs no lock: the rings and tables it touches are reserved
+    lk.unlock();
+    cudaSetDevice(s->device);
+    // index span (one or two copies: the ring may have skipped to its start)
+    const int64_t lo = b->idx_begin % s->idx_cap, n = b->idx_end - b->idx_begin;
+    if (n > 0) {
+        if (lo + n <= s->idx_cap) {
+            cudaMemcpyAsync(s->idx_dev + lo, s->idx_host + lo, sizeof(int64_t) * n,
+                            cudaMemcpyHostToDevice, s->stream);
+        } else {
+            cudaMemcpyAsync(s->idx_dev + lo, s->idx_host + lo, sizeof(int64_t) * (s->idx_cap - lo),
+                            cudaMemcpyHostToDevice, s->stream);
+            cudaMemcpyAsync(s->idx_dev, s->idx_host, sizeof(int64_t) * (n - (s->idx_cap - lo)),
+                            cudaMemcpyHostToDevice, s->stream);
+        }
+    }
+    cudaMemcpyAsync(td, th, kTableHeader + sizeof(ibp_request) * recs.size(),
+                    cudaMemcpyHostToDevice, s->stream);
+    ibp_status st = ibp_batch_fetch(s->registry, reinterpret_cast<const ibp_request *>(td + kTableHeader),
+                                    reinterpret_cast<const int32_t *>(td), s->max_batch, s->ws,
+                                    kStatusBytes, s->stream);
+    cudaLaunchHostFunc(s->stream, batch_done, new DoneCtx{s, b});
+    lk.lock();
+    if (st != IBP_OK) s->err = ibp_last_error();
+    return true;
+}
+
+static void scheduler(Server *s) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        retire(s);
+        bool launched = false;
+        if ((int)s->inflight.size() < s->max_inflight && !s->pending.empty())
+            launched = launch_batch_locked(s, lk);
+        if (!launched) s->cv.wait_for(lk, std::chrono::milliseconds(5));
+    }
+}
+
+}  // namespace ibp200
+
+using namespace ibp200;
+
+extern "C" {
+
+ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int32_t nsets,
+                             int word_bytes, void *out_arena, size_t arena_bytes,
+                             int64_t index_capacity, int32_t max_batch, int32_t max_inflight,
+                             ibp_server **out) {
+    clear_error();
+    IBP_ARG(registry && sets && nsets > 0 && out_arena && out, "server_create: null argument");
+    IBP_ARG(word_bytes == 4 || word_bytes == 8, "server_create: word size must be 4 or 8");
+    IBP_ARG(max_batch > 0 && max_batch <= 8192, "server_create: max_batch must be 1..8192");
+    IBP_ARG(max_inflight >= 1 && max_inflight <= 8, "server_create: max_inflight must be 1..8");
+    IBP_ARG(index_capacity > 0, "server_create: index capacity must be positive");
+    Server *s = new Server();
+    s->registry = registry;
+    for (int i = 0; i < nsets; ++i) {
+        s->set_v.push_back(sets[i].vec_size);
+        s->set_n.push_back(sets[i].num_vecs);
+    }
+    s->word_bytes = word_bytes;
+    s->max_batch = max_batch;
+    s->max_inflight = max_inflight;
+    s->arena = (char *)out_arena;
+    s->arena_bytes = arena_bytes;
+    s->free_list[0] = (int64_t)(arena_bytes / 256 * 256);
+    s->idx_cap = index_capacity;
+    cudaGetDevice(&s->device);
+    auto fail = [&](cudaError_t e, const char *what) {
+        set_error("server_create: %s: %s", what, cudaGetErrorString(e));
+        return IBP_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaHostAlloc(&s->idx_host, sizeof(int64_t) * index_capacity, cudaHostAllocDefault)) != cudaSuccess) return fail(e, "index staging");
+    if ((e = cudaMalloc(&s->idx_dev, sizeof(int64_t) * index_capacity)) != cudaSuccess) return fail(e, "device index ring");
+    const size_t tbytes = kTableHeader + sizeof(ibp_request) * max_batch;
+    for (int i = 0; i < max_inflight; ++i) {
+        char *h = nullptr, *d = nullptr;
+        if ((e = cudaHostAlloc(&h, tbytes, cudaHostAllocDefault)) != cudaSuccess) return fail(e, "table");
+        if ((e = cudaMalloc(&d, tbytes)) != cudaSuccess) return fail(e, "table");
+        s->tbl_host.push_back(h);
+        s->tbl_dev.push_back(d);
+        s->tbl_busy.push_back(false);
+    }
+    if ((e = cudaMalloc(&s->ws, kStatusBytes)) != cudaSuccess) return fail(e, "workspace");
+    s->thr = std::thread(scheduler, s);
+    *out = reinterpret_cast<ibp_server *>(s);
+    return IBP_OK;
+}
+
+// Queue a request: `count` rows of set `set`, either the listed rows (host array `rows`,
+// copied before this returns) or, with rows == NULL, rows first .. first+count-1.  Returns
+// its id in *id.  IBP_ERR_WORKSPACE when the index staging is full (retry later) or the
+// request could never fit the output arena.
+ibp_status ibp_server_submit(ibp_server *srv, int32_t set, const int64_t *rows, int64_t first,
+                             int64_t count, int64_t *id) {
+    clear_error();
+    Server *s = reinterpret_cast<Server *>(srv);
+    IBP_ARG(s && id, "server_submit: null argument");
+    IBP_ARG(set >= 0 && set < (int32_t)s->set_v.size(), "server_submit: no set %d", set);
+    IBP_ARG(count > 0, "server_submit: count must be positive");
+    const int64_t out_bytes = count * s->set_v[set] * s->word_bytes;
+    if ((size_t)out_bytes > s->arena_bytes) {
+        set_error("server_submit: %lld output bytes exceed the %zu-byte arena", (long long)out_bytes,
+                  s->arena_bytes);
+        return IBP_ERR_WORKSPACE;
+    }
+    std::unique_lock<std::mutex> lk(s->mu);
+    SrvRequest r{};
+    r.id = s->next_id++;
+    r.set = set;
+    r.count = count;
+    r.first = first;
+    r.has_index = rows != nullptr;
+    r.idx_off = -1;
+    r.out_off = -1;
+    r.out_bytes = out_bytes;
+    r.t_submit = now_us();
+    if (rows) {
+        retire(s);
+        const int64_t pos = ring_reserve(s, count);
+        if (pos < 0) {
+            set_error("server_submit: index staging full (%lld of %lld entries in use)",
+                      (long long)ring_used(s), (long long)s->idx_cap);
+            return IBP_ERR_WORKSPACE;
+        }
+        std::memcpy(s->idx_host + pos, rows, sizeof(int64_t) * count);
+        r.idx_off = pos;
+    }
+    r.ring_end = s->idx_head;
+    s->reqs[r.id] = r;
+    s->pending.push_back(r.id);
+    *id = r.id;
+    lk.unlock();
+    s->cv.notify_all();
+    return IBP_OK;
+}
+
+// Wait (up to timeout_ms; < 0 forever) for request `id`; on success *out is its output rows
+// (device memory, count x vec_size words) and times[0..2] = submit, admit, done (host
+// microseconds, steady clock).  IBP_ERR_UNSUPPORTED on timeout.
+ibp_status ibp_server_wait(ibp_server *srv, int64_t id, int32_t timeout_ms, void **out,
+                           double *times) {
+    clear_error();
+    Server *s = reinterpret_cast<Server *>(srv);
+    IBP_ARG(s, "server_wait: null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto ready = [&] {
+        auto it = s->reqs.find(id);
+        return it == s->reqs.end() || it->second.done;
+    };
+    if (timeout_ms < 0)
+        s->done_cv.wait(lk, ready);
+    else if (!s->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+        set_error("server_wait: request %lld not done within %d ms", (long long)id, timeout_ms);
+        return IBP_ERR_UNSUPPORTED;
+    }
+    auto it = s->reqs.find(id);
+    IBP_ARG(it != s->reqs.end(), "server_wait: unknown request %lld", (long long)id);
+    if (out) *out = s->arena + it->second.out_off;
+    if (times) {
+        times[0] = it->second.t_submit;
+        times[1] = it->second.t_admit;
+        times[2] = it->second.t_done;
+    }
+    if (!s->err.empty()) {
+        set_error("server: %s", s->err.c_str());
+        return IBP_ERR_CUDA;
+    }
+    return IBP_OK;
+}
+
+// Return a finished request's output rows to the arena.
+ibp_status ibp_server_release(ibp_server *srv, int64_t id) {
+    clear_error();
+    Server *s = reinterpret_cast<Server *>(srv);
+    IBP_ARG(s, "server_release: null server");
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        auto it = s->reqs.find(id);
+        IBP_ARG(it != s->reqs.end() && it->second.done, "server_release: request %lld is not done",
+                (long long)id);
+        arena_free(s, it->second.out_off, it->second.out_bytes);
+        s->reqs.erase(it);
+    }
+    s->cv.notify_all();
+    return IBP_OK;
+}
+
+// stats[0..3] = batches launched, rows done, output bytes done, requests pending.
+ibp_status ibp_server_stats(ibp_server *srv, int64_t *stats) {
+    Server *s = reinterpret_cast<Server *>(srv);
+    if (!s || !stats) return IBP_ERR_ARGUMENT;
+    std::lock_guard<std::mutex> g(s->mu);
+    stats[0] = s->batches;
+    stats[1] = s->rows_done;
+    stats[2] = s->bytes_done;
+    stats[3] = (int64_t)s->pending.size();
+    return IBP_OK;
+}
+
+// Stop the scheduler after the in-flight batches finish and free the server's buffers.
+ibp_status ibp_server_destroy(ibp_server *srv) {
+    Server *s = reinterpret_cast<Server *>(srv);
+    if (!s) return IBP_OK;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->thr.joinable()) s->thr.join();
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (size_t i = 0; i < s->tbl_host.size(); ++i) {
+        cudaFreeHost(s->tbl_host[i]);
+        cudaFree(s->tbl_dev[i]);
+    }
+    cudaFreeHost(s->idx_host);
+    cudaFree(s->idx_dev);
+    cudaFree(s->ws);
+    cudaStreamDestroy(s->stream);
+    for (Batch *b : s->inflight) delete b;
+    delete s;
+    return IBP_OK;
+}
+
+}  // extern "C"
