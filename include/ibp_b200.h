@@ -67,7 +67,8 @@ unsigned long long ibp_kernel_launch_count(void);
 
 /* Device status word of the last call that used `workspace`: bit 0 = an index was out of
  * range; bit 1 = a row marked compressed has a bitmap whose stream would not fit the row
- * (the bitmask/mask do not belong to the data), and its output row was left untouched.
+ * (the bitmask/mask do not belong to the data), and its output row was left untouched;
+ * bit 2 = a sorted batch's request counts did not add up to its stated total_rows.
  * Enqueues a copy on `stream` and waits for it (blocking). */
 ibp_status ibp_read_status(const void *workspace, int32_t *status, ibp_stream_t stream);
 
@@ -180,7 +181,8 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
  *      ibp_batch_fetch.  It reads both on the device, so a CUDA graph that captured the call
  *      can be replayed after the caller rewrites the records (e.g. with a copy node).
  * Out-of-range rows or set ids set bit 0 of the status word (first 4 bytes of the workspace).
- * Rows are fetched as listed (no de-duplication inside a request). */
+ * Rows are fetched as listed (no de-duplication inside a request; ibp_batch_fetch_sorted
+ * below de-duplicates). */
 typedef struct {
     const void *comp;       /* compressed rows, device or pinned host memory */
     int64_t num_vecs;
@@ -217,14 +219,29 @@ ibp_status ibp_batch_autotune(const void *registry, const ibp_request *requests,
                               const int32_t *num_requests, int32_t max_requests,
                               void *workspace, size_t workspace_bytes, int32_t *chosen,
                               ibp_stream_t stream);
+/* De-duplicating batch: like ibp_batch_fetch, but each request's rows are radix-sorted on the
+ * device first, so a row listed several times in one request crosses the bus once and is
+ * copied into its other output rows, and the fetch walks each set in row order (the per-call
+ * path of ibp_decompress_fetch does the same).  num_requests (1..8192) and total_rows (the sum
+ * of the requests' counts, < 2^31) are host values, so a graph that captured the call serves
+ * batches of exactly that shape only.  `requests` is device memory.  If the device counts
+ * disagree with total_rows, bit 2 of the status word is set and only positions below the
+ * smaller total are fetched.  Workspace: ibp_batch_fetch_sorted_workspace_size(max rows,
+ * max requests) bytes; the status word is its first 4 bytes. */
+size_t ibp_batch_fetch_sorted_workspace_size(int64_t max_total_rows, int32_t max_requests);
+ibp_status ibp_batch_fetch_sorted(const void *registry, const ibp_request *requests,
+                                  int32_t num_requests, int64_t total_rows, void *workspace,
+                                  size_t workspace_bytes, ibp_stream_t stream);
 
 /* ---------------------------------------------------------------- serving
  * No counterpart in the reference (its callers issue one decompress_fetch per lookup).  A
  * continuous-batching server over a registry: clients submit requests from any thread; a
  * scheduler thread admits them in arrival order whenever their output fits the caller's
- * device arena, packs all admitted requests into one batched launch, and keeps up to
- * max_inflight launches on the GPU, so requests arriving meanwhile join the next launch.
- * Buffers (index staging rings of index_capacity entries, request tables, a stream) are
+ * device arena, packs all admitted requests into one de-duplicating batched launch
+ * (ibp_batch_fetch_sorted; a batch holds at most max(index_capacity, 2^20) rows, and a
+ * single range request above that is fetched unsorted), and keeps up to max_inflight
+ * launches on the GPU, so requests arriving meanwhile join the next launch.  Buffers (index
+ * staging rings of index_capacity entries, request tables, the sort workspace, a stream) are
  * allocated at creation only.  Timestamps are host steady-clock microseconds. */
 typedef struct ibp_server ibp_server;
 ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int32_t nsets,
@@ -242,6 +259,12 @@ ibp_status ibp_server_wait(ibp_server *srv, int64_t id, int32_t timeout_ms, void
 /* Give a finished request's output rows back to the arena. */
 ibp_status ibp_server_release(ibp_server *srv, int64_t id);
 /* stats[0..3] = batches launched, rows done, output bytes done, requests pending. */
+/* Admission limits of one batch: at most max_rows rows (no more than the sort workspace's
+ * max(index_capacity, 2^20)) and max_bytes output bytes, both counted after the batch's
+ * first request, which is always admitted.  <= 0 keeps the current value.  Defaults: the
+ * sort workspace's rows and 128 MiB.  Smaller batches finish early requests of a burst
+ * sooner (lower p50); larger ones amortise per-launch cost. */
+ibp_status ibp_server_set_batch_limits(ibp_server *srv, int64_t max_rows, int64_t max_bytes);
 ibp_status ibp_server_stats(ibp_server *srv, int64_t *stats);
 ibp_status ibp_server_destroy(ibp_server *srv);
 

@@ -4,6 +4,7 @@
     bf = BatchFetcher(reg, max_requests=64)
     outs = bf.fetch([(set_id, index_tensor_or_None, first, count), ...])
     bf.capture()     # later fetches replay one CUDA graph: copy of the request table + launch
+    outs = bf.fetch(reqs, dedup=True)   # sort + de-duplicate each request's rows first
 
 The request table (count + ibp_request records) is written into a pinned host buffer and
 copied to the device inside the captured work, so one graph serves any batch of up to
@@ -76,6 +77,8 @@ class BatchFetcher:
         self.graphs = None
         self.turn = 0
         self.keep = [None] * buffers
+        self.sort_ws = None
+        self.last_ws = self.ws
 
     def _write(self, b, requests, outs):
         if len(requests) > self.max:
@@ -108,17 +111,37 @@ class BatchFetcher:
         return [torch.empty((int(rq[3]), self.reg.vec_sizes[int(rq[0])]), dtype=self.reg.dtype,
                             device=device) for rq in requests]
 
-    def fetch(self, requests, outs=None):
-        """requests: (set id, int64 CUDA index or None, first row, row count) each."""
+    def _launch_sorted(self, b, nreq, rows):
+        need = _lib.ibp_batch_fetch_sorted_workspace_size(rows, nreq)
+        if self.sort_ws is None or self.sort_ws.numel() < need:
+            self.sort_ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+        d = self.dev[b]
+        d.copy_(self.host[b], non_blocking=True)
+        _capi.check(_lib.ibp_batch_fetch_sorted(self.reg.buf.data_ptr(), d.data_ptr() + _HDR, nreq,
+                                                rows, self.sort_ws.data_ptr(),
+                                                self.sort_ws.numel(), _stream()))
+        self.last_ws = self.sort_ws
+
+    def fetch(self, requests, outs=None, dedup=False):
+        """requests: (set id, int64 CUDA index or None, first row, row count) each.
+
+        dedup=True sorts each request's rows on the device and fetches a repeated row once
+        (ibp_batch_fetch_sorted); it runs outside the captured graphs, whose table shape is
+        fixed at capture."""
         requests = [(s, (None if i is None else i.to(torch.int64)), f, c) for s, i, f, c in requests]
         if outs is None:
             outs = self.outputs_for(requests)
         b = self.turn
         self.turn = (self.turn + 1) % len(self.host)
         self._write(b, requests, outs)
-        if self.graphs is not None:
+        if dedup:
+            if requests:
+                self._launch_sorted(b, len(requests), sum(max(int(r[3]), 0) for r in requests))
+        elif self.graphs is not None:
+            self.last_ws = self.ws
             self.graphs[b].replay()
         else:
+            self.last_ws = self.ws
             self._launch(b)
         ev = torch.cuda.Event()
         ev.record()
@@ -156,6 +179,7 @@ class BatchFetcher:
         return {"threads": chosen[0], "rows_in_flight": chosen[1], "blocks_per_sm": chosen[2]}
 
     def status(self):
-        """Device status word of the last batch (bit 0: a bad row index or set id)."""
+        """Device status word of the last batch (bit 0: a bad row index or set id; bit 1: a
+        corrupt row; bit 2: request counts that disagree with a sorted batch's total)."""
         torch.cuda.synchronize()
-        return int(self.ws[:4].view(torch.int32).item())
+        return int(self.last_ws[:4].view(torch.int32).item())

@@ -7,6 +7,8 @@
 //
 // The reference fetches one set per decompress_fetch call (src/decompress.cu:10-156); its
 // embedding-bag and decoder-layer callers issue one call per table or tensor.
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -24,6 +26,7 @@ struct RegistryHeader {
     int32_t nsets;
     int32_t word_bytes;
     int64_t max_v;
+    int64_t max_n;           // most rows of any set
     int32_t host_resident;   // set 0 lives in host memory
     int32_t ratio_bucket;    // mean first-read fraction of the rows, in tenths
 };
@@ -57,46 +60,74 @@ __host__ __device__ inline size_t batch_head_bytes(int max_req) {
     return align_up(sizeof(int64_t) * ((size_t)max_req + 1 + 256), 16);
 }
 
-// Units of 32 rows: request r owns units [prefix[r], prefix[r+1]).
+// Exclusive scan of the requests' unit counts into prefix[0..nreq], for any block size:
+// each thread sums a contiguous segment of requests, thread 0 scans the per-thread sums
+// (part[], blockDim.x entries), each thread then writes its segment.  The rows per unit
+// (unit_positions of the batch's total rows over the grid's warps) is returned; every block
+// computes the same.
+template <typename Req>
+__device__ __forceinline__ int unit_prefix(const Req *reqs, int nreq, int64_t *prefix,
+                                           int64_t *part) {
+    const int per = (nreq + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int r0 = (int)threadIdx.x * per;
+    int64_t rows = 0;
+    for (int r = r0; r < r0 + per && r < nreq; ++r) rows += max(reqs[r].count, (int64_t)0);
+    part[threadIdx.x] = rows;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t run = 0;
+        for (int t = 0; t < (int)blockDim.x; ++t) run += part[t];
+        prefix[nreq] = run;
+    }
+    __syncthreads();
+    const int upos = unit_positions(prefix[nreq], (int64_t)gridDim.x * (blockDim.x >> 5));
+    int64_t sum = 0;
+    for (int r = r0; r < r0 + per && r < nreq; ++r) {
+        const int64_t cnt = reqs[r].count;
+        sum += cnt > 0 ? (cnt + upos - 1) / upos : 0;
+    }
+    __syncthreads();  // every thread has read the row total
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t run = 0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            const int64_t x = part[t];
+            part[t] = run;
+            run += x;
+        }
+        prefix[nreq] = run;
+    }
+    __syncthreads();
+    int64_t excl = part[threadIdx.x];
+    for (int r = r0; r < r0 + per && r < nreq; ++r) {
+        prefix[r] = excl;
+        const int64_t cnt = reqs[r].count;
+        excl += cnt > 0 ? (cnt + upos - 1) / upos : 0;
+    }
+    __syncthreads();
+    return upos;
+}
+
+// The request owning unit u: the last r with prefix[r] <= u.
+__device__ __forceinline__ int unit_owner(const int64_t *prefix, int nreq, int64_t u) {
+    int lo = 0, hi = nreq - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Units of `upos` rows: request r owns units [prefix[r], prefix[r+1]).
 template <typename U, int NC>
-__global__ void __launch_bounds__(256) batch_fetch_kernel(BatchArgs<U> a) {
+__global__ void __launch_bounds__(256, 2) batch_fetch_kernel(BatchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     int64_t *prefix = reinterpret_cast<int64_t *>(smem);
     U *slots = reinterpret_cast<U *>(smem + batch_head_bytes(a.max_req)) +
                (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
     const int nreq = min(max(*a.nreq, 0), a.max_req);
-    // exclusive scan of the requests' unit counts, for any block size: each thread sums a
-    // contiguous segment of requests, thread 0 scans the per-thread sums, each thread then
-    // writes its segment's prefixes
-    {
-        int64_t *part = prefix + a.max_req + 1;  // blockDim.x partial sums
-        const int per = (nreq + (int)blockDim.x - 1) / (int)blockDim.x;
-        const int r0 = (int)threadIdx.x * per;
-        int64_t sum = 0;
-        for (int r = r0; r < r0 + per && r < nreq; ++r) {
-            const int64_t cnt = a.reqs[r].count;
-            sum += cnt > 0 ? (cnt + 31) / 32 : 0;
-        }
-        part[threadIdx.x] = sum;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int64_t run = 0;
-            for (int t = 0; t < (int)blockDim.x; ++t) {
-                const int64_t x = part[t];
-                part[t] = run;
-                run += x;
-            }
-            prefix[nreq] = run;
-        }
-        __syncthreads();
-        int64_t excl = part[threadIdx.x];
-        for (int r = r0; r < r0 + per && r < nreq; ++r) {
-            prefix[r] = excl;
-            const int64_t cnt = a.reqs[r].count;
-            excl += cnt > 0 ? (cnt + 31) / 32 : 0;
-        }
-        __syncthreads();
-    }
+    const int upos = unit_prefix(a.reqs, nreq, prefix, prefix + a.max_req + 1);
     const int lane = threadIdx.x & 31;
     const int64_t total_units = prefix[nreq];
     LaneTables<U, NC> lt;
@@ -106,14 +137,9 @@ __global__ void __launch_bounds__(256) batch_fetch_kernel(BatchArgs<U> a) {
         if (lane == 0) u = atomicAdd(a.work, 1ull);
         u = __shfl_sync(0xffffffffu, u, 0);
         if ((int64_t)u >= total_units) break;
-        // request owning unit u: the last r with prefix[r] <= u
-        int lo = 0, hi = nreq - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (prefix[mid] <= (int64_t)u) lo = mid; else hi = mid - 1;
-        }
+        const int lo = unit_owner(prefix, nreq, (int64_t)u);
         const RequestDev rq = a.reqs[lo];
-        const int64_t k = ((int64_t)u - prefix[lo]) * 32 + lane;
+        const int64_t k = ((int64_t)u - prefix[lo]) * upos + lane;
         const bool set_ok = rq.set >= 0 && rq.set < a.nsets;
         if (!set_ok) {
             if (lane == 0) atomicOr(a.status, kStatusBadIndex);
@@ -124,7 +150,7 @@ __global__ void __launch_bounds__(256) batch_fetch_kernel(BatchArgs<U> a) {
             lt.load(s.t, s.v);
             cur_set = rq.set;
         }
-        const bool valid = k < rq.count;
+        const bool valid = lane < upos && k < rq.count;
         const int64_t key = valid ? (rq.index ? rq.index[k] : rq.first + k) : -1;
         const bool bad = valid && (key < 0 || key >= s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
@@ -190,6 +216,7 @@ static ibp_status register_sets(const ibp_set_desc *sets, int nsets, void *reg, 
             return IBP_ERR_WORKSPACE;
         }
         h.max_v = std::max<int64_t>(h.max_v, d.vec_size);
+        h.max_n = std::max<int64_t>(h.max_n, d.num_vecs);
         ratio += d.vec_size > 0 ? (double)s.first_words / (double)d.vec_size : 1.0;
         if (d.vec_size > 0) IBP_RET(build_tables<U>((const U *)d.mask, (const U *)d.bitval, d.vec_size, s.t, st));
     }
@@ -288,6 +315,282 @@ static ibp_status read_header(const void *reg, RegistryHeader &h) {
         return IBP_ERR_ARGUMENT;
     }
     h = it->second;
+    return IBP_OK;
+}
+
+
+// ------------------------------------------------------------------ sorted batches
+// Positions p of a sorted batch run over the requests' rows back to back: request r owns
+// [rowpre[r], rowpre[r+1]).  The caller states the total; positions at or past it are not
+// fetched, and a table whose counts disagree with it is flagged (kStatusBadTable).
+
+__global__ void batch_rowpre_kernel(const RequestDev *__restrict__ reqs, int nreq, int64_t total,
+                                    int64_t *__restrict__ rowpre, int32_t *__restrict__ status) {
+    __shared__ int64_t part[256];
+    const int per = (nreq + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int r0 = (int)threadIdx.x * per;
+    int64_t sum = 0;
+    for (int r = r0; r < r0 + per && r < nreq; ++r) sum += max(reqs[r].count, (int64_t)0);
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t run = 0;
+        for (int t = 0; t < (int)blockDim.x; ++t) {
+            const int64_t x = part[t];
+            part[t] = run;
+            run += x;
+        }
+        rowpre[nreq] = run;
+        if (run != total) atomicOr(status, kStatusBadTable);
+    }
+    __syncthreads();
+    int64_t excl = part[threadIdx.x];
+    for (int r = r0; r < r0 + per && r < nreq; ++r) {
+        rowpre[r] = excl;
+        excl += max(reqs[r].count, (int64_t)0);
+    }
+}
+
+// Keys are (r << rb) | row, with an out-of-range row replaced by the set's row count and an
+// unknown set by all ones in the row field, so one radix sort orders every request's rows
+// and keeps requests apart.  Positions past the table's own total sort last (all ones).
+template <typename U>
+__global__ void batch_keys_kernel(const RowSet<U> *__restrict__ sets, int nsets,
+                                  const RequestDev *__restrict__ reqs, int nreq,
+                                  const int64_t *__restrict__ rowpre, int64_t total, int rb,
+                                  int kb, int64_t *__restrict__ keys, int64_t *__restrict__ vals) {
+    const int64_t have = rowpre[nreq];
+    const int64_t rmask = ((int64_t)1 << rb) - 1;
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total;
+         p += (int64_t)gridDim.x * blockDim.x) {
+        vals[p] = p;
+        if (p >= have) {
+            keys[p] = ((int64_t)1 << kb) - 1;
+            continue;
+        }
+        int lo = 0, hi = nreq - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (rowpre[mid] <= p) lo = mid; else hi = mid - 1;
+        }
+        const RequestDev &q = reqs[lo];
+        const int64_t k = p - rowpre[lo];
+        int64_t row = rmask;
+        if (q.set >= 0 && q.set < nsets) {
+            const int64_t r = q.index ? q.index[k] : q.first + k;
+            const int64_t n = sets[q.set].n;
+            row = (r >= 0 && r < n) ? r : n;
+        }
+        keys[p] = ((int64_t)lo << rb) | row;
+    }
+}
+
+template <typename U>
+struct SortedArgs {
+    const RowSet<U> *sets;
+    int32_t nsets;
+    const RequestDev *reqs;
+    int32_t nreq;
+    const int64_t *rowpre;   // device, nreq + 1
+    int64_t total;           // positions sorted
+    const int64_t *keys;     // sorted composite keys
+    const int64_t *vals;     // their batch positions
+    int rb;
+    unsigned long long *work;
+    int32_t *status;
+    int64_t slot_words;
+    int slots;
+};
+
+// Distinct (request, row) keys of each request's sorted segment are fetched and decoded
+// into the request's output; repeats are left to fill_repeats_kernel.
+template <typename U, int NC>
+__global__ void __launch_bounds__(256, 2) batch_fetch_sorted_kernel(SortedArgs<U> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int64_t *prefix = reinterpret_cast<int64_t *>(smem);
+    U *slots = reinterpret_cast<U *>(smem + batch_head_bytes(a.nreq)) +
+               (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
+    const int upos = unit_prefix(a.reqs, a.nreq, prefix, prefix + a.nreq + 1);
+    const int lane = threadIdx.x & 31;
+    const int64_t total_units = prefix[a.nreq];
+    const int64_t rmask = ((int64_t)1 << a.rb) - 1;
+    LaneTables<U, NC> lt;
+    int cur_set = -1;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(a.work, 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if ((int64_t)u >= total_units) break;
+        const int r = unit_owner(prefix, a.nreq, (int64_t)u);
+        const RequestDev rq = a.reqs[r];
+        const int64_t c0 = ((int64_t)u - prefix[r]) * upos;  // first row of the unit
+        const bool set_ok = rq.set >= 0 && rq.set < a.nsets;
+        if (!set_ok) {
+            if (lane == 0) atomicOr(a.status, kStatusBadIndex);
+            continue;
+        }
+        const RowSet<U> &s = a.sets[rq.set];
+        if (NC > 0 && rq.set != cur_set) {
+            lt.load(s.t, s.v);
+            cur_set = rq.set;
+        }
+        const int64_t p0 = a.rowpre[r] + c0;
+        const bool valid = lane < upos && c0 + lane < rq.count && p0 + lane < a.total;
+        const int64_t key = valid ? a.keys[p0 + lane] : -1;
+        int64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+        if (lane == 0) prev = (c0 > 0 && valid) ? a.keys[p0 - 1] : key - 1;
+        const int64_t row = key & rmask;
+        bool head = valid && key != prev;
+        const bool bad = head && row >= s.n;
+        if (bad) atomicOr(a.status, kStatusBadIndex);
+        head = head && !bad;
+        U *orow = reinterpret_cast<U *>(rq.out) +
+                  (head ? (a.vals[p0 + lane] - a.rowpre[r]) : 0) * s.v;
+        const bool packed = head && ((__ldg(&s.bitmask[row >> 5]) >> (row & 31)) & 1);
+        fetch_heads<U, NC>(s, lt, slots, a.slots, a.slot_words, row, orow, head, packed,
+                           a.status);
+    }
+}
+
+// Output rows of a sorted batch: position k (key (r << rb) | row) goes to row
+// vals[k] - rowpre[r] of request r's output.
+template <typename U>
+struct BatchRows {
+    const RowSet<U> *sets;
+    int32_t nsets;
+    const RequestDev *reqs;
+    int32_t nreq;
+    const int64_t *rowpre;
+    const int64_t *vals;
+    int rb;
+    __device__ __forceinline__ bool valid(int64_t key) const {
+        if ((key >> rb) >= nreq) return false;
+        const RequestDev &q = reqs[key >> rb];
+        return q.set >= 0 && q.set < nsets && (key & (((int64_t)1 << rb) - 1)) < sets[q.set].n;
+    }
+    __device__ __forceinline__ U *row(int64_t k, int64_t key) const {
+        const int r = (int)(key >> rb);
+        return reinterpret_cast<U *>(reqs[r].out) + (vals[k] - rowpre[r]) * sets[reqs[r].set].v;
+    }
+    __device__ __forceinline__ int64_t words(int64_t key) const {
+        return sets[reqs[key >> rb].set].v;
+    }
+};
+
+static int bits_for(int64_t x) {  // bits to hold 0..x
+    int b = 1;
+    while (b < 62 && ((int64_t)1 << b) <= x) ++b;
+    return b;
+}
+
+static size_t sorted_temp_bytes(int64_t rows) {
+    size_t temp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, temp, (const int64_t *)nullptr, (int64_t *)nullptr,
+                                    (const int64_t *)nullptr, (int64_t *)nullptr,
+                                    (int)std::max<int64_t>(rows, 1), 0, 63);
+    return temp;
+}
+
+static size_t sorted_workspace(int64_t rows, int32_t max_req) {
+    Sizer z;
+    z.take<char>(kStatusBytes);
+    z.take<int64_t>((size_t)max_req + 1);  // row prefix
+    for (int i = 0; i < 4; ++i) z.take<int64_t>((size_t)std::max<int64_t>(rows, 1));
+    z.take<char>(sorted_temp_bytes(rows));
+    return z.total();
+}
+
+template <typename U, int NC>
+static ibp_status launch_sorted_nc(SortedArgs<U> a, int64_t max_v, Shape sh, cudaStream_t st) {
+    const size_t slot_bytes = (size_t)a.slot_words * sizeof(U);
+    const size_t head = batch_head_bytes(a.nreq);
+    int threads = sh.threads;
+    int slots = std::max(1, std::min(sh.slots, kRowsInFlight));
+    const int maxs = device_max_smem_optin();
+    while (slots > 1 && head + slot_bytes * slots * (threads / 32) > 96 * 1024) --slots;
+    while (threads > 32 && head + slot_bytes * slots * (threads / 32) > (size_t)maxs) threads -= 32;
+    const size_t smem = head + slot_bytes * slots * (threads / 32);
+    if ((int64_t)smem > maxs) {
+        set_error("batch_fetch_sorted: %d requests and rows of %lld words do not fit shared memory",
+                  a.nreq, (long long)max_v);
+        return IBP_ERR_UNSUPPORTED;
+    }
+    a.slots = slots;
+    auto kern = batch_fetch_sorted_kernel<U, NC>;
+    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    if (per_sm < 1) per_sm = 1;
+    if (sh.occupancy > 0 && sh.occupancy < per_sm) per_sm = sh.occupancy;
+    const int pslot = profile_begin(st);
+    kern<<<device_sm_count() * per_sm, threads, smem, st>>>(a);
+    IBP_LAUNCHED("batch_fetch_sorted_kernel");
+    profile_end(pslot, st);
+    return IBP_OK;
+}
+
+template <typename U>
+static ibp_status launch_sorted(const void *reg, const RegistryHeader &h, const RequestDev *dreqs,
+                                int nreq, int64_t rows, void *ws, size_t ws_bytes, Shape sh,
+                                cudaStream_t st) {
+    const size_t need = sorted_workspace(rows, nreq);
+    if (!ws || ws_bytes < need) {
+        set_error("batch_fetch_sorted: workspace of %zu bytes is below the required %zu for %lld "
+                  "rows", ws_bytes, need, (long long)rows);
+        return IBP_ERR_WORKSPACE;
+    }
+    const int rb = bits_for(std::max<int64_t>(h.max_n, 1));
+    const int kb = rb + bits_for(nreq);
+    if (kb > 62) {
+        set_error("batch_fetch_sorted: %d requests over sets of %lld rows exceed the sort key",
+                  nreq, (long long)h.max_n);
+        return IBP_ERR_UNSUPPORTED;
+    }
+    Carver c{(char *)reg, 0, (size_t)-1};
+    c.take<RegistryHeader>(1);
+    const RowSet<U> *sets = c.take<RowSet<U>>((size_t)h.nsets);
+    Carver w{(char *)ws, 0, ws_bytes};
+    int32_t *status = w.take<int32_t>(kStatusBytes / 4);
+    int64_t *rowpre = w.take<int64_t>((size_t)nreq + 1);
+    int64_t *keys_in = w.take<int64_t>((size_t)std::max<int64_t>(rows, 1));
+    int64_t *vals_in = w.take<int64_t>((size_t)std::max<int64_t>(rows, 1));
+    int64_t *keys = w.take<int64_t>((size_t)std::max<int64_t>(rows, 1));
+    int64_t *vals = w.take<int64_t>((size_t)std::max<int64_t>(rows, 1));
+    size_t temp_bytes = sorted_temp_bytes(rows);
+    void *temp = w.take<char>(temp_bytes);
+    IBP_CUDA(cudaMemsetAsync(status, 0, 128, st));
+    batch_rowpre_kernel<<<1, 256, 0, st>>>(dreqs, nreq, rows, rowpre, status);
+    IBP_LAUNCHED("batch_rowpre_kernel");
+    if (rows == 0) return IBP_OK;
+    const int blocks = (int)std::min<int64_t>((rows + 255) / 256, 4096);
+    batch_keys_kernel<U><<<blocks, 256, 0, st>>>(sets, h.nsets, dreqs, nreq, rowpre, rows, rb, kb,
+                                                 keys_in, vals_in);
+    IBP_LAUNCHED("batch_keys_kernel");
+    IBP_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys, vals_in, vals,
+                                             (int)rows, 0, kb, st));
+    SortedArgs<U> a{};
+    a.sets = sets;
+    a.nsets = h.nsets;
+    a.reqs = dreqs;
+    a.nreq = nreq;
+    a.rowpre = rowpre;
+    a.total = rows;
+    a.keys = keys;
+    a.vals = vals;
+    a.rb = rb;
+    a.work = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 64);
+    a.status = status;
+    a.slot_words = (int64_t)align_up((size_t)h.max_v + 2, 16 / sizeof(U));
+    if (h.max_v > 64)
+        IBP_RET((launch_sorted_nc<U, 0>(a, h.max_v, sh, st)));
+    else if (h.max_v > 32)
+        IBP_RET((launch_sorted_nc<U, 2>(a, h.max_v, sh, st)));
+    else
+        IBP_RET((launch_sorted_nc<U, 1>(a, h.max_v, sh, st)));
+    const int64_t fb = std::min<int64_t>((rows + 255) / 256, (int64_t)device_sm_count() * 8);
+    BatchRows<U> br{sets, h.nsets, dreqs, nreq, rowpre, vals, rb};
+    fill_repeats_kernel<U, BatchRows<U>><<<(unsigned)fb, 256, 0, st>>>(keys, rows, br);
+    IBP_LAUNCHED("fill_repeats_kernel(batch)");
     return IBP_OK;
 }
 
@@ -414,6 +717,37 @@ ibp_status ibp_batch_autotune(const void *registry, const ibp_request *requests,
     IBP_DPRINTF("[ibp] batch autotune: threads %d, rows in flight %d, blocks/SM %d (%.3f ms)\n",
                 best_sh.threads, best_sh.slots, best_sh.occupancy, best / 2);
     return IBP_OK;
+}
+
+size_t ibp_batch_fetch_sorted_workspace_size(int64_t max_total_rows, int32_t max_requests) {
+    if (max_total_rows < 0 || max_total_rows > INT32_MAX || max_requests < 1) return 0;
+    return sorted_workspace(max_total_rows, max_requests);
+}
+
+ibp_status ibp_batch_fetch_sorted(const void *registry, const ibp_request *requests,
+                                  int32_t num_requests, int64_t total_rows, void *workspace,
+                                  size_t workspace_bytes, ibp_stream_t stream) {
+    clear_error();
+    IBP_ARG(registry && requests, "batch_fetch_sorted: null argument");
+    IBP_ARG(num_requests > 0 && num_requests <= 8192,
+            "batch_fetch_sorted: num_requests must be 1..8192");
+    IBP_ARG(total_rows >= 0 && total_rows <= INT32_MAX,
+            "batch_fetch_sorted: total_rows must be 0..2^31-1");
+    RegistryHeader h{};
+    IBP_RET(read_header(registry, h));
+    Shape sh;
+    {
+        std::lock_guard<std::mutex> g(g_shape_mu);
+        auto it = g_shapes.find(ShapeKey{h.word_bytes, h.max_v, h.ratio_bucket, h.host_resident});
+        if (it != g_shapes.end()) sh = it->second;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const RequestDev *dreqs = reinterpret_cast<const RequestDev *>(requests);
+    if (h.word_bytes == 8)
+        return launch_sorted<uint64_t>(registry, h, dreqs, num_requests, total_rows, workspace,
+                                       workspace_bytes, sh, st);
+    return launch_sorted<uint32_t>(registry, h, dreqs, num_requests, total_rows, workspace,
+                                   workspace_bytes, sh, st);
 }
 
 }  // extern "C"

@@ -45,11 +45,12 @@ struct FetchArgs {
     unsigned long long *work;  // chunk counter, zero at launch
     int64_t slot_words;   // shared-memory words per row slot
     int slots;            // row slots per warp (<= kRowsInFlight)
+    int upos;             // positions per chunk (unit_positions: 4..32)
 };
 
 // ------------------------------------------------------------------ fetch kernel
 template <typename U, int NC>
-__global__ void __launch_bounds__(kFetchThreads) fetch_rows_kernel(FetchArgs<U> a) {
+__global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     U *slots = reinterpret_cast<U *>(smem) + (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
@@ -59,11 +60,11 @@ __global__ void __launch_bounds__(kFetchThreads) fetch_rows_kernel(FetchArgs<U> 
         unsigned long long chunk = 0;
         if (lane == 0) chunk = atomicAdd(a.work, 1ull);
         chunk = __shfl_sync(0xffffffffu, chunk, 0);
-        const int64_t k0 = (int64_t)chunk * 32;
+        const int64_t k0 = (int64_t)chunk * a.upos;
         if (k0 >= a.nrows) break;
-        // lane-parallel metadata of the chunk's 32 positions
+        // lane-parallel metadata of the chunk's positions
         const int64_t k = k0 + lane;
-        const bool valid = k < a.nrows;
+        const bool valid = lane < a.upos && k < a.nrows;
         const int64_t key = valid ? (a.keys ? a.keys[k] : k) : -1;
         bool head = valid;
         if (a.dedup) {
@@ -83,92 +84,16 @@ __global__ void __launch_bounds__(kFetchThreads) fetch_rows_kernel(FetchArgs<U> 
 }
 
 // ------------------------------------------------------------------ repeats
-// First position of `target` in the sorted keys[0..hi] (keys[hi] == target): a 32-way
-// search, one probe per lane per round.
-__device__ __forceinline__ int64_t first_occurrence(const int64_t *__restrict__ keys, int64_t hi,
-                                                    int64_t target) {
-    const int lane = threadIdx.x & 31;
-    int64_t lo = 0;  // invariant: keys[lo - 1] < target (or lo == 0), keys[hi] == target
-    while (lo < hi) {
-        const int64_t step = (hi - lo + 31) / 32;
-        int64_t p = lo + (int64_t)lane * step;
-        if (p > hi) p = hi;
-        const unsigned less = __ballot_sync(0xffffffffu, keys[p] < target);
-        const int cnt = __popc(less);
-        if (cnt == 0) break;
-        const int64_t plast = lo + (int64_t)(cnt - 1) * step;
-        if (cnt < 32) {
-            const int64_t pnext = lo + (int64_t)cnt * step;
-            if (pnext < hi) hi = pnext;
-        }
-        lo = plast + 1;
-    }
-    return lo;
-}
-
-// Every position whose key repeats the previous one gets a copy of the output row decoded
-// for the first position of its run.  A warp takes 32 positions; each distinct source row
-// is read once and written to all of its positions in the chunk.
+// Output rows of the per-call fetch: position k goes to row pos[k] of `out`.
 template <typename U>
-__global__ void __launch_bounds__(256)
-fill_repeats_kernel(const int64_t *__restrict__ keys, const int64_t *__restrict__ pos,
-                    int64_t nrows, int64_t n, int64_t v, U *__restrict__ out) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const bool vec = (((uintptr_t)out) & 15) == 0 && ((v * (int64_t)sizeof(U)) & 15) == 0;
-    for (int64_t k0 = warp * 32; k0 < nrows; k0 += nwarps * 32) {
-        const int64_t k = k0 + lane;
-        const bool valid = k < nrows;
-        const int64_t key = valid ? keys[k] : -1;
-        int64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-        if (lane == 0) prev = k0 > 0 ? keys[k0 - 1] : key - 1;
-        const bool head = valid && key != prev;
-        const unsigned hb = __ballot_sync(0xffffffffu, head);
-        if (__ballot_sync(0xffffffffu, valid && !head) == 0) continue;
-        // run start of the chunk's first position when its run began in an earlier chunk
-        int64_t h0 = k0;
-        if (!(hb & 1u)) h0 = first_occurrence(keys, k0, __shfl_sync(0xffffffffu, key, 0));
-        const unsigned below = hb & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));
-        const int64_t h = below ? k0 + (31 - __clz(below)) : h0;
-        const bool dup = valid && !head && key >= 0 && key < n;
-        const int64_t d = dup ? pos[k] : 0;
-        unsigned dm = __ballot_sync(0xffffffffu, dup);
-        while (dm) {
-            const int64_t hs = __shfl_sync(0xffffffffu, h, __ffs(dm) - 1);
-            const unsigned same = __ballot_sync(0xffffffffu, dup && h == hs) & dm;
-            dm &= ~same;
-            const U *src = out + pos[hs] * v;
-            if (vec) {
-                const int64_t n16 = v * (int64_t)sizeof(U) / 16;
-                for (int64_t q0 = 0; q0 < n16; q0 += 32) {
-                    const int64_t q = q0 + lane;
-                    uint4 x = make_uint4(0, 0, 0, 0);
-                    if (q < n16) x = reinterpret_cast<const uint4 *>(src)[q];
-                    unsigned m = same;
-                    while (m) {
-                        const int j = __ffs(m) - 1;
-                        m &= m - 1;
-                        const int64_t dj = __shfl_sync(0xffffffffu, d, j);
-                        if (q < n16) reinterpret_cast<uint4 *>(out + dj * v)[q] = x;
-                    }
-                }
-            } else {
-                for (int64_t w0 = 0; w0 < v; w0 += 32) {
-                    const int64_t w = w0 + lane;
-                    const U x = w < v ? src[w] : (U)0;
-                    unsigned m = same;
-                    while (m) {
-                        const int j = __ffs(m) - 1;
-                        m &= m - 1;
-                        const int64_t dj = __shfl_sync(0xffffffffu, d, j);
-                        if (w < v) out[dj * v + w] = x;
-                    }
-                }
-            }
-        }
-    }
-}
+struct CallRows {
+    U *out;
+    const int64_t *pos;
+    int64_t v, n;
+    __device__ __forceinline__ bool valid(int64_t key) const { return key >= 0 && key < n; }
+    __device__ __forceinline__ U *row(int64_t k, int64_t) const { return out + pos[k] * v; }
+    __device__ __forceinline__ int64_t words(int64_t) const { return v; }
+};
 
 // Sort inputs: positions 0..nrows-1, and the keys with every out-of-range index replaced by
 // n, so that the radix sort over the bits of n orders all keys exactly (the fetch kernel
@@ -240,7 +165,8 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
         if (per_sm < 1) per_sm = 1;
         blocks = (int64_t)device_sm_count() * per_sm;
     }
-    const int64_t chunks = (a.nrows + 31) / 32;
+    a.upos = unit_positions(a.nrows, blocks * (threads / 32));
+    const int64_t chunks = (a.nrows + a.upos - 1) / a.upos;
     const int64_t need = (chunks + threads / 32 - 1) / (threads / 32);
     if (blocks > need) blocks = need;
     const int slot = profile_begin(st);
@@ -318,7 +244,8 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     int64_t fb = (nidx + 255) / 256;
     const int64_t cap = (int64_t)device_sm_count() * 8;
     if (fb > cap) fb = cap;
-    fill_repeats_kernel<U><<<(unsigned)fb, 256, 0, st>>>(keys, pos, nidx, n, v, out);
+    fill_repeats_kernel<U, CallRows<U>><<<(unsigned)fb, 256, 0, st>>>(keys, nidx,
+                                                                       CallRows<U>{out, pos, v, n});
     IBP_LAUNCHED("fill_repeats_kernel");
     return IBP_OK;
 }

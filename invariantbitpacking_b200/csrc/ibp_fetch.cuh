@@ -11,6 +11,16 @@ namespace ibp200 {
 
 constexpr int kRowsInFlight = 4;  // first reads a warp keeps outstanding
 
+// Positions a warp takes per unit of work: 32 (lane-parallel metadata over the full warp)
+// unless the fetch has too few rows to give every warp of the grid a unit; then fewer, down
+// to 4, so a small fetch spreads over more warps (each warp's rows form a chain of dependent
+// reads, a few microseconds each over PCIe).
+__host__ __device__ __forceinline__ int unit_positions(int64_t rows, int64_t warps) {
+    int u = 32;
+    while (u > 4 && (int64_t)(u / 2) * warps >= rows) u >>= 1;
+    return u;
+}
+
 // One tensor set as the fetch kernels see it.
 template <typename U>
 struct RowSet {
@@ -147,9 +157,10 @@ __device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t 
 
 
 // Fetch and decode (or copy, when not packed) the rows of the lanes whose `head` is set:
-// groups of up to `nslots` rows have their first reads loaded into registers together (16-
-// byte loads, all rows before any store), so their PCIe or HBM round trips overlap; rows
-// that are not 16-byte aligned or whose first read exceeds 1 KiB take a plain loop.
+// groups of up to `nslots` rows have their first reads, and then the rest of the rows that
+// need it, loaded into registers together (16-byte loads, all rows before any store), so
+// their PCIe or HBM round trips overlap; rows that are not 16-byte aligned, whose first
+// read exceeds 1 KiB or whose tail exceeds 512 bytes take a plain loop.
 // `orow` is each lane's output row.
 template <typename U, int NC>
 __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables<U, NC> &lt,
@@ -203,34 +214,161 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
             }
         }
         __syncwarp();
+        // exact lengths from the bitmaps, then the rest of every row that needs more than its
+        // first read, all issued before any is waited for (16-byte blocks in registers, at
+        // most 32 per row; longer tails and unaligned rows take the plain loop)
+        int64_t end[kRowsInFlight];
+        {
+            constexpr int per16 = 16 / sizeof(U);
+            uint4 tail[kRowsInFlight];
+            int64_t tb0[kRowsInFlight], tb1[kRowsInFlight];
+#pragma unroll
+            for (int q = 0; q < kRowsInFlight; ++q) {
+                end[q] = -1;
+                tb0[q] = tb1[q] = 0;
+                if (q < cnt && __shfl_sync(0xffffffffu, (int)packed, lid[q])) {
+                    const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+                    const U *row = s.comp + r * v;
+                    U *buf = slots + q * slot_words;
+                    end[q] = row_words<U, NC>(buf, v, s.mw, s.t, lt);
+                    if (end[q] < v && end[q] > s.first_words) {
+                        const int64_t b0 = s.first_words / per16;
+                        const int64_t b1 = (end[q] + per16 - 1) / per16;
+                        if ((((uintptr_t)row) & 15) == 0 && b1 - b0 <= 32) {
+                            tb0[q] = b0;
+                            tb1[q] = b1;
+                            if (b0 + lane < b1)
+                                tail[q] = reinterpret_cast<const uint4 *>(row)[b0 + lane];
+                        } else {
+                            issue_words<U>(buf, row, s.first_words, end[q]);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kRowsInFlight; ++q)
+                if (tb0[q] + lane < tb1[q])
+                    reinterpret_cast<uint4 *>(slots + q * slot_words)[tb0[q] + lane] = tail[q];
+        }
+        __syncwarp();
 #pragma unroll
         for (int q = 0; q < kRowsInFlight; ++q) {
             if (q < cnt) {
                 const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
                 U *o = reinterpret_cast<U *>(
                     __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
-                const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[q]);
-                const U *row = s.comp + r * v;
-                if (!pk) {
-                    warp_copy<U>(o, row, v);
+                if (end[q] < 0) {
+                    warp_copy<U>(o, s.comp + r * v, v);
                     continue;
                 }
-                U *buf = slots + q * slot_words;
-                const int64_t end = row_words<U, NC>(buf, v, s.mw, s.t, lt);
-                if (end >= v) {
+                if (end[q] >= v) {
                     // a bitmap claiming a stream as long as the raw row cannot come from this
                     // mask: report it and leave the output row alone
                     if (lane == 0) atomicOr(status, kStatusCorruptRow);
                     continue;
                 }
-                if (end > s.first_words) issue_words<U>(buf, row, s.first_words, end);
-                __syncwarp();
+                U *buf = slots + q * slot_words;
                 // words past the stream read as zero (get_bits looks one word ahead; the
                 // value there never reaches an output bit)
-                if (lane < 2) buf[end + lane] = 0;
+                if (lane < 2) buf[end[q] + lane] = 0;
                 __syncwarp();
                 decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
                 __syncwarp();
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ repeats
+// First position of `target` in the sorted keys[0..hi] (keys[hi] == target): a 32-way
+// search, one probe per lane per round.
+__device__ __forceinline__ int64_t first_occurrence(const int64_t *__restrict__ keys, int64_t hi,
+                                                    int64_t target) {
+    const int lane = threadIdx.x & 31;
+    int64_t lo = 0;  // invariant: keys[lo - 1] < target (or lo == 0), keys[hi] == target
+    while (lo < hi) {
+        const int64_t step = (hi - lo + 31) / 32;
+        int64_t p = lo + (int64_t)lane * step;
+        if (p > hi) p = hi;
+        const unsigned less = __ballot_sync(0xffffffffu, keys[p] < target);
+        const int cnt = __popc(less);
+        if (cnt == 0) break;
+        const int64_t plast = lo + (int64_t)(cnt - 1) * step;
+        if (cnt < 32) {
+            const int64_t pnext = lo + (int64_t)cnt * step;
+            if (pnext < hi) hi = pnext;
+        }
+        lo = plast + 1;
+    }
+    return lo;
+}
+
+// Every position whose (sorted) key repeats the previous one gets a copy of the output row
+// decoded for the first position of its run.  A warp takes 32 positions; each distinct
+// source row is read once and written to all of its positions in the chunk.  `Rows` maps a
+// position and its key to its output row (valid(key), row(k, key), words(key)).
+template <typename U, typename Rows>
+__global__ void __launch_bounds__(256)
+fill_repeats_kernel(const int64_t *__restrict__ keys, int64_t nrows, Rows rows) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k0 = warp * 32; k0 < nrows; k0 += nwarps * 32) {
+        const int64_t k = k0 + lane;
+        const bool valid = k < nrows;
+        const int64_t key = valid ? keys[k] : -1;
+        int64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+        if (lane == 0) prev = k0 > 0 ? keys[k0 - 1] : key - 1;
+        const bool head = valid && key != prev;
+        const unsigned hb = __ballot_sync(0xffffffffu, head);
+        if (__ballot_sync(0xffffffffu, valid && !head) == 0) continue;
+        // run start of the chunk's first position when its run began in an earlier chunk
+        int64_t h0 = k0;
+        if (!(hb & 1u)) h0 = first_occurrence(keys, k0, __shfl_sync(0xffffffffu, key, 0));
+        const unsigned below = hb & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));
+        const int64_t h = below ? k0 + (31 - __clz(below)) : h0;
+        const bool dup = valid && !head && rows.valid(key);
+        U *d = dup ? rows.row(k, key) : nullptr;
+        unsigned dm = __ballot_sync(0xffffffffu, dup);
+        while (dm) {
+            const int leader = __ffs(dm) - 1;
+            const int64_t hs = __shfl_sync(0xffffffffu, h, leader);
+            const int64_t ks = __shfl_sync(0xffffffffu, key, leader);
+            const unsigned same = __ballot_sync(0xffffffffu, dup && h == hs) & dm;
+            dm &= ~same;
+            const U *src = rows.row(hs, ks);
+            const int64_t v = rows.words(ks);
+            const bool aligned = (((uintptr_t)d) & 15) == 0;
+            const bool vec = (((uintptr_t)src) & 15) == 0 && ((v * (int64_t)sizeof(U)) & 15) == 0 &&
+                             (__ballot_sync(0xffffffffu, (same >> lane & 1u) && !aligned) == 0);
+            if (vec) {
+                const int64_t n16 = v * (int64_t)sizeof(U) / 16;
+                for (int64_t q0 = 0; q0 < n16; q0 += 32) {
+                    const int64_t q = q0 + lane;
+                    uint4 x = make_uint4(0, 0, 0, 0);
+                    if (q < n16) x = reinterpret_cast<const uint4 *>(src)[q];
+                    unsigned m = same;
+                    while (m) {
+                        const int j = __ffs(m) - 1;
+                        m &= m - 1;
+                        U *dj = reinterpret_cast<U *>(
+                            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(d), j));
+                        if (q < n16) reinterpret_cast<uint4 *>(dj)[q] = x;
+                    }
+                }
+            } else {
+                for (int64_t w0 = 0; w0 < v; w0 += 32) {
+                    const int64_t w = w0 + lane;
+                    const U x = w < v ? src[w] : (U)0;
+                    unsigned m = same;
+                    while (m) {
+                        const int j = __ffs(m) - 1;
+                        m &= m - 1;
+                        U *dj = reinterpret_cast<U *>(
+                            __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(d), j));
+                        if (w < v) dj[w] = x;
+                    }
+                }
             }
         }
     }

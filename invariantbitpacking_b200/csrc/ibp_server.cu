@@ -2,17 +2,19 @@
 //
 // Clients submit requests (registered set, host row list, count) from any thread; a
 // scheduler thread admits them in arrival order as output memory frees up, packs every
-// admitted request into one batched launch (ibp_batch_fetch over the set registry), and
+// admitted request into one batched launch (ibp_batch_fetch_sorted over the set registry:
+// every request's rows sorted and de-duplicated on the device), and
 // keeps up to `max_inflight` batches on the GPU at once, so requests that arrive while
 // others run join the next launch instead of waiting for the queue to drain.  Completion is
-// stamped by a host callback queued behind each batch (no polling).
+// stamped by a thread that waits on each batch's event in launch order.
 //
 // Memory (all reserved at creation, nothing allocated per request):
 //   * output arena: the caller's device buffer; a first-fit free list with coalescing hands
 //     each request its rows, which stay valid until the client releases the request;
 //   * index staging: a pinned host ring and a device ring of the same size; submit copies the
 //     client's row list into the host ring, the batch copies its span to the device ring;
-//   * request tables: one pinned + one device table per in-flight batch.
+//   * request tables: one pinned + one device table per in-flight batch;
+//   * one sort workspace for max(index capacity, 2^20) rows (batches run in stream order).
 //
 // The reference has no serving layer: its callers (ColossalAI embedding bags, FlexGen
 // layers, DGL samplers) call decompress_fetch once per lookup.
@@ -57,6 +59,7 @@ struct Batch {
     std::vector<int64_t> ids;
     int64_t idx_begin = 0, idx_end = 0;  // index-ring span [begin, end), monotonic positions
     int table = 0;
+    bool recorded = false;  // its completion event is in the stream
     bool complete = false;
 };
 
@@ -75,25 +78,34 @@ struct Server {
     int64_t idx_cap = 0, idx_head = 0, idx_tail = 0, idx_launched = 0;
     std::vector<char *> tbl_host, tbl_dev;
     std::vector<bool> tbl_busy;
+    std::vector<cudaEvent_t> tbl_event;  // completion event of the batch using each table
     void *ws = nullptr;
+    size_t ws_bytes = 0;
+    int64_t sort_cap = 0;  // rows a de-duplicating batch may hold (workspace size)
+    int64_t batch_rows = 0, batch_bytes = 0;  // admission limits of one batch
     cudaStream_t stream = nullptr;
     int device = 0;
 
     std::mutex mu;
     std::condition_variable cv;       // scheduler wake-ups
     std::condition_variable done_cv;  // client waits
+    std::condition_variable rec_cv;   // completion thread: a batch's event was recorded
     std::deque<int64_t> pending;
     std::map<int64_t, SrvRequest> reqs;
     std::deque<Batch *> inflight;
     int64_t next_id = 1;
     bool stop = false;
-    std::thread thr;
+    std::thread thr, done_thr;
     std::string err;
     // stats
     int64_t batches = 0, rows_done = 0, bytes_done = 0;
 };
 
 static constexpr int kTableHeader = 64;
+// Output bytes one batch admits by default (after its first request): ~2 ms of transfer at
+// host-link speed, so a burst is served in arrival order by a pipeline of short launches
+// instead of one launch that completes every request at its end.
+static constexpr int64_t kDefaultBatchBytes = 128ll << 20;
 
 // ---------------------------------------------------------------- arena allocation
 static int64_t arena_alloc(Server *s, int64_t bytes) {
@@ -143,31 +155,43 @@ static int64_t ring_reserve(Server *s, int64_t n) {
     return pos;
 }
 
-// ---------------------------------------------------------------- completion callback
-struct DoneCtx {
-    Server *s;
-    Batch *b;
-};
-
-static void CUDART_CB batch_done(void *p) {
-    DoneCtx *c = static_cast<DoneCtx *>(p);
-    const double t = now_us();
-    {
-        std::lock_guard<std::mutex> g(c->s->mu);
-        for (int64_t id : c->b->ids) {
-            auto it = c->s->reqs.find(id);
-            if (it != c->s->reqs.end()) {
+// ---------------------------------------------------------------- completion thread
+// Waits for each batch's event in launch order and stamps its requests done.  An event
+// rather than a host callback in the stream, so the next batch starts on the GPU without
+// waiting for a host thread.
+static void completer(Server *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        Batch *b = nullptr;
+        s->rec_cv.wait(lk, [&] {
+            for (Batch *x : s->inflight)
+                if (!x->complete) {
+                    b = x->recorded ? x : nullptr;
+                    return b != nullptr;
+                }
+            return s->stop;
+        });
+        if (!b) break;  // stopping and nothing left in flight
+        const cudaEvent_t ev = s->tbl_event[b->table];
+        lk.unlock();
+        const cudaError_t e = cudaEventSynchronize(ev);
+        const double t = now_us();
+        lk.lock();
+        if (e != cudaSuccess && s->err.empty()) s->err = cudaGetErrorString(e);
+        for (int64_t id : b->ids) {
+            auto it = s->reqs.find(id);
+            if (it != s->reqs.end()) {
                 it->second.t_done = t;
                 it->second.done = true;
-                c->s->rows_done += it->second.count;
-                c->s->bytes_done += it->second.out_bytes;
+                s->rows_done += it->second.count;
+                s->bytes_done += it->second.out_bytes;
             }
         }
-        c->b->complete = true;
+        b->complete = true;
+        s->cv.notify_all();
+        s->done_cv.notify_all();
     }
-    c->s->cv.notify_all();
-    c->s->done_cv.notify_all();
-    delete c;
 }
 
 // ---------------------------------------------------------------- scheduler
@@ -195,10 +219,15 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
     b->idx_begin = s->idx_launched;
     b->idx_end = s->idx_launched;
     std::vector<ibp_request> recs;
+    int64_t rows = 0, out_bytes = 0;
     // admit in arrival order while the output fits (head-of-line: an oversized request
-    // waits for memory, later ones wait behind it to keep arrival order)
+    // waits for memory, later ones wait behind it to keep arrival order) and the rows fit
+    // one de-duplicating batch
     while (!s->pending.empty() && (int)recs.size() < s->max_batch) {
         SrvRequest &r = s->reqs[s->pending.front()];
+        if (!recs.empty() &&
+            (rows + r.count > s->batch_rows || out_bytes + r.out_bytes > s->batch_bytes))
+            break;
         const int64_t off = arena_alloc(s, r.out_bytes);
         if (off < 0) break;
         r.out_off = off;
@@ -210,6 +239,8 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
         q.count = r.count;
         q.out = s->arena + off;
         recs.push_back(q);
+        rows += r.count;
+        out_bytes += r.out_bytes;
         b->ids.push_back(r.id);
         b->idx_end = std::max(b->idx_end, r.ring_end);
         s->pending.pop_front();
@@ -243,12 +274,20 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
     }
     cudaMemcpyAsync(td, th, kTableHeader + sizeof(ibp_request) * recs.size(),
                     cudaMemcpyHostToDevice, s->stream);
-    ibp_status st = ibp_batch_fetch(s->registry, reinterpret_cast<const ibp_request *>(td + kTableHeader),
-                                    reinterpret_cast<const int32_t *>(td), s->max_batch, s->ws,
-                                    kStatusBytes, s->stream);
-    cudaLaunchHostFunc(s->stream, batch_done, new DoneCtx{s, b});
+    // a batch that fits the sort workspace is de-duplicated and fetched in row order; a
+    // single range request beyond it (already in row order, no repeats) goes unsorted
+    const ibp_request *dreq = reinterpret_cast<const ibp_request *>(td + kTableHeader);
+    ibp_status st =
+        rows <= s->sort_cap
+            ? ibp_batch_fetch_sorted(s->registry, dreq, (int32_t)recs.size(), rows, s->ws,
+                                     s->ws_bytes, s->stream)
+            : ibp_batch_fetch(s->registry, dreq, reinterpret_cast<const int32_t *>(td),
+                              s->max_batch, s->ws, s->ws_bytes, s->stream);
+    cudaEventRecord(s->tbl_event[table], s->stream);
     lk.lock();
     if (st != IBP_OK) s->err = ibp_last_error();
+    b->recorded = true;
+    s->rec_cv.notify_all();
     return true;
 }
 
@@ -309,9 +348,18 @@ ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int
         s->tbl_host.push_back(h);
         s->tbl_dev.push_back(d);
         s->tbl_busy.push_back(false);
+        cudaEvent_t ev = nullptr;
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+        s->tbl_event.push_back(ev);
     }
-    if ((e = cudaMalloc(&s->ws, kStatusBytes)) != cudaSuccess) return fail(e, "workspace");
+    s->sort_cap = std::min<int64_t>(std::max<int64_t>(index_capacity, 1 << 20), INT32_MAX);
+    s->batch_rows = s->sort_cap;
+    s->batch_bytes = kDefaultBatchBytes;
+    s->ws_bytes = std::max<size_t>(ibp_batch_fetch_sorted_workspace_size(s->sort_cap, max_batch),
+                                   ibp_batch_fetch_workspace_size());
+    if ((e = cudaMalloc(&s->ws, s->ws_bytes)) != cudaSuccess) return fail(e, "workspace");
     s->thr = std::thread(scheduler, s);
+    s->done_thr = std::thread(completer, s);
     *out = reinterpret_cast<ibp_server *>(s);
     return IBP_OK;
 }
@@ -415,6 +463,18 @@ ibp_status ibp_server_release(ibp_server *srv, int64_t id) {
     return IBP_OK;
 }
 
+// Admission limits of one batch: at most max_rows rows (capped by the sort workspace) and
+// max_bytes output bytes after its first request; <= 0 keeps the current value.
+ibp_status ibp_server_set_batch_limits(ibp_server *srv, int64_t max_rows, int64_t max_bytes) {
+    clear_error();
+    Server *s = reinterpret_cast<Server *>(srv);
+    IBP_ARG(s, "server_set_batch_limits: null server");
+    std::lock_guard<std::mutex> g(s->mu);
+    if (max_rows > 0) s->batch_rows = std::min(max_rows, s->sort_cap);
+    if (max_bytes > 0) s->batch_bytes = max_bytes;
+    return IBP_OK;
+}
+
 // stats[0..3] = batches launched, rows done, output bytes done, requests pending.
 ibp_status ibp_server_stats(ibp_server *srv, int64_t *stats) {
     Server *s = reinterpret_cast<Server *>(srv);
@@ -437,12 +497,15 @@ ibp_status ibp_server_destroy(ibp_server *srv) {
     }
     s->cv.notify_all();
     if (s->thr.joinable()) s->thr.join();
+    s->rec_cv.notify_all();
+    if (s->done_thr.joinable()) s->done_thr.join();
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->stream);
     for (size_t i = 0; i < s->tbl_host.size(); ++i) {
         cudaFreeHost(s->tbl_host[i]);
         cudaFree(s->tbl_dev[i]);
     }
+    for (cudaEvent_t ev : s->tbl_event) cudaEventDestroy(ev);
     cudaFreeHost(s->idx_host);
     cudaFree(s->idx_dev);
     cudaFree(s->ws);

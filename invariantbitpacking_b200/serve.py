@@ -7,8 +7,9 @@
     ... use out ...
     srv.release(rid)                # rows go back to the arena
 
-Requests are admitted in arrival order as their output fits the arena; every admitted
-request joins the next batched launch, with up to `max_inflight` launches on the GPU.
+Requests are admitted in arrival order as their output fits the arena and join the next
+batched launch (de-duplicated, up to the batch limits: 128 MiB of output by default), with
+up to `max_inflight` launches on the GPU.
 """
 import ctypes
 
@@ -22,7 +23,7 @@ _lib = _capi.lib
 
 class Server:
     def __init__(self, registry, arena_bytes, index_capacity=1 << 25, max_batch=256,
-                 max_inflight=2):
+                 max_inflight=2, batch_bytes=None, batch_rows=None):
         self.reg = registry
         self.arena = torch.empty(int(arena_bytes), dtype=torch.uint8, device="cuda")
         self.handle = ctypes.c_void_p()
@@ -31,6 +32,13 @@ class Server:
             self.arena.data_ptr(), self.arena.numel(), int(index_capacity), int(max_batch),
             int(max_inflight), ctypes.byref(self.handle)))
         self.counts = {}
+        if batch_bytes is not None or batch_rows is not None:
+            self.set_batch_limits(batch_rows, batch_bytes)
+
+    def set_batch_limits(self, rows=None, nbytes=None):
+        """Cap one batch at `rows` rows and `nbytes` output bytes (None: keep)."""
+        _capi.check(_lib.ibp_server_set_batch_limits(self.handle, int(rows or 0),
+                                                     int(nbytes or 0)))
 
     def submit(self, set_id, rows=None, first=0, count=None):
         """Queue `rows` (host int64 array) or rows first .. first+count-1 of a set."""

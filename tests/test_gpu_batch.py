@@ -112,3 +112,92 @@ def test_batch_bad_rows_and_sets_are_flagged(ibp, sets):
     o2 = torch.zeros((2, 32), dtype=torch.int64, device="cuda")
     bf.fetch([(7, None, 0, 2)], [o2])
     assert bf.status() & 1 and not o2.any()
+
+
+def dup_requests(rng, sets, k):
+    """Requests whose rows repeat heavily (a few hundred distinct rows per request)."""
+    reqs = []
+    for j in range(k):
+        sid = int(rng.integers(0, len(sets)))
+        n = sets[sid][0].shape[0]
+        if j % 5 == 4:
+            first = int(rng.integers(0, n // 2))
+            reqs.append((sid, None, first, int(rng.integers(0, n - first))))
+        else:
+            cnt = int(rng.integers(1, 4000))
+            hot = rng.integers(0, n, int(rng.integers(1, 300)))
+            reqs.append((sid, torch.from_numpy(hot[rng.integers(0, hot.size, cnt)]).cuda(), 0, cnt))
+    return reqs
+
+
+def test_batch_sorted_dedup_matches_sources(ibp, sets):
+    from invariantbitpacking_b200.batch import BatchFetcher, SetRegistry
+    reg = SetRegistry([s[1] for s in sets])
+    bf = BatchFetcher(reg, max_requests=64)
+    rng = np.random.default_rng(11)
+    for k in (1, 7, 40, 64):
+        reqs = dup_requests(rng, sets, k)
+        outs = bf.fetch(reqs, dedup=True)
+        check(outs, reqs, sets)
+        assert bf.status() == 0
+    # the same requests through the listed-order path agree
+    reqs = dup_requests(rng, sets, 30)
+    a = bf.fetch(reqs, dedup=True)
+    torch.cuda.synchronize()
+    b = bf.fetch(reqs)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+
+
+def test_batch_sorted_after_capture_and_bad_rows(ibp, sets):
+    from invariantbitpacking_b200.batch import BatchFetcher, SetRegistry
+    reg = SetRegistry([s[1] for s in sets[:2]])
+    bf = BatchFetcher(reg, max_requests=8)
+    bf.capture()
+    good = torch.tensor([2, 0, 2, 1, 0], dtype=torch.int64, device="cuda")
+    bad = torch.tensor([1, 10 ** 9, -5, 1, 10 ** 9], dtype=torch.int64, device="cuda")
+    o2 = torch.zeros((2, 32), dtype=torch.int64, device="cuda")
+    reqs = [(0, good, 0, 5), (1, bad, 0, 5), (7, None, 0, 2), (1, None, 0, 0)]
+    outs = bf.outputs_for([reqs[0], reqs[1]]) + [o2] + bf.outputs_for([reqs[3]])
+    outs = bf.fetch(reqs, outs, dedup=True)
+    torch.cuda.synchronize()
+    assert bf.status() & 1
+    assert np.array_equal(outs[0].cpu().numpy(), sets[0][0][[2, 0, 2, 1, 0]])
+    o = outs[1].cpu().numpy()
+    assert np.array_equal(o[0], sets[1][0][1]) and np.array_equal(o[3], sets[1][0][1])
+    assert outs[3].shape[0] == 0 and not o2.any()
+    # graph replays still serve the listed-order path afterwards
+    outs = bf.fetch([(0, good, 0, 5)])
+    check(outs, [(0, good, 0, 5)], sets)
+
+
+def test_batch_sorted_total_mismatch_is_flagged(ibp, sets):
+    import ctypes
+    from invariantbitpacking_b200 import _capi
+    from invariantbitpacking_b200.batch import SetRegistry
+    reg = SetRegistry([s[1] for s in sets[:1]])
+    idx = torch.arange(0, 600, 3, dtype=torch.int64, device="cuda")
+    out = torch.zeros((200, 32), dtype=torch.int64, device="cuda")
+    rec = (_capi.Request * 1)()
+    rec[0].set, rec[0].index, rec[0].first, rec[0].count, rec[0].out = 0, idx.data_ptr(), 0, 200, out.data_ptr()
+    dreq = torch.frombuffer(bytearray(bytes(rec)), dtype=torch.uint8).cuda()
+    lib = _capi.lib
+    for total in (150, 260):
+        ws = torch.empty(lib.ibp_batch_fetch_sorted_workspace_size(total, 1), dtype=torch.uint8,
+                         device="cuda")
+        out.zero_()
+        _capi.check(lib.ibp_batch_fetch_sorted(reg.buf.data_ptr(), dreq.data_ptr(), 1, total,
+                                               ws.data_ptr(), ws.numel(),
+                                               torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        assert int(ws[:4].view(torch.int32).item()) & 4
+        got = out.cpu().numpy()
+        want = sets[0][0][idx.cpu().numpy()]
+        k = min(total, 200)
+        assert np.array_equal(got[:k], want[:k])
+        assert not got[k:].any()
+    with pytest.raises(_capi.IBPError):
+        _capi.check(lib.ibp_batch_fetch_sorted(reg.buf.data_ptr(), dreq.data_ptr(), 1, 100,
+                                               ws.data_ptr(), 16,
+                                               torch.cuda.current_stream().cuda_stream))

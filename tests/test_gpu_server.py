@@ -1,6 +1,7 @@
 """Continuous-batching server: a burst of mixed requests from two client threads, with an
-output arena small enough that admission has to wait for releases; every result must equal
-the same request fetched alone by plain decompress_fetch, and the source rows."""
+output arena small enough that admission has to wait for releases, rows that repeat inside
+a request, with the default batch limits and with small ones; every result must equal the
+same request fetched alone by plain decompress_fetch, and the source rows."""
 import threading
 
 import numpy as np
@@ -18,7 +19,8 @@ def ibp():
     return m
 
 
-def test_server_results_equal_solo_fetches(ibp):
+@pytest.mark.parametrize("limits", [None, (2000, 256 << 10)])
+def test_server_results_equal_solo_fetches(ibp, limits):
     from invariantbitpacking_b200.batch import SetRegistry
     from invariantbitpacking_b200.serve import Server
     rng = np.random.default_rng(5)
@@ -35,6 +37,8 @@ def test_server_results_equal_solo_fetches(ibp):
     reg = SetRegistry(sets)
     srv = Server(reg, arena_bytes=64 << 20, index_capacity=1 << 20, max_batch=16,
                  max_inflight=2)
+    if limits:
+        srv.set_batch_limits(*limits)
     reqs = []
     for j in range(60):
         sid = int(rng.integers(0, 4))
@@ -44,6 +48,9 @@ def test_server_results_equal_solo_fetches(ibp):
             first = int(rng.integers(0, n - cnt)) if cnt < n else 0
             cnt = min(cnt, n - first)
             reqs.append((sid, None, first, cnt))
+        elif j % 4 == 2:  # rows repeat: a few dozen hot rows
+            hot = rng.integers(0, n, int(rng.integers(1, 40))).astype(np.int64)
+            reqs.append((sid, hot[rng.integers(0, hot.size, cnt)], 0, cnt))
         else:
             reqs.append((sid, rng.integers(0, n, cnt).astype(np.int64), 0, cnt))
     ids = [None] * len(reqs)
@@ -79,4 +86,8 @@ def test_server_results_equal_solo_fetches(ibp):
     st = srv.stats()
     assert st["rows_done"] == sum(r[3] for r in reqs) and st["pending"] == 0
     assert st["batches"] < len(reqs)  # requests were batched
+    if limits:
+        big = max(r[3] * sets[r[0]][0].shape[1] * 8 for r in reqs)
+        assert st["batches"] >= sum(r[3] * sets[r[0]][0].shape[1] * 8 for r in reqs) // (
+            limits[1] + big)
     srv.close()
