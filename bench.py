@@ -37,7 +37,7 @@ METRIC = "decompress_fetch delivered GB/s (graph features, Zipf 1.1 mini-batches
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--rows", type=int, default=ROWS)
@@ -85,7 +85,9 @@ def max_over_ranks(x, ws):
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples (every 20 ms) during the timed region: the sampler is running, with
+    its first sample in, before the region starts; samples outside the region are dropped
+    (a region shorter than one period keeps the sample nearest to its middle)."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -95,6 +97,7 @@ class Clocks:
         self.index = index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -104,17 +107,22 @@ class Clocks:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 5.0
+            while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.005)
         except Exception:
             self.proc = None
+        self.t0 = time.monotonic()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *a):
+        self.t1 = time.monotonic()
         if self.proc:
-            time.sleep(0.25)
+            time.sleep(0.05)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -124,22 +132,30 @@ class Clocks:
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        rows = []
+        for t, ln in self.lines:
             p = [q.strip() for q in ln.split(",")]
             if len(p) < 7:
                 continue
             try:
-                sm.append(float(p[0]))
-                mx = max(mx, float(p[1]))
+                rows.append((t, float(p[0]), float(p[1]), p[3:7]))
             except ValueError:
                 continue
-            for nm, val in zip(names, p[3:7]):
+        if not rows or self.t0 is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        t1 = self.t1 if self.t1 is not None else rows[-1][0]
+        inside = [r for r in rows if self.t0 <= r[0] <= t1 + 0.02]
+        if not inside:
+            mid = 0.5 * (self.t0 + t1)
+            inside = [min(rows, key=lambda r: abs(r[0] - mid))]
+        for t, clk, cmax, flags in inside:
+            sm.append(clk)
+            mx = max(mx, cmax)
+            for nm, val in zip(names, flags):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "region_ms": round((t1 - self.t0) * 1e3, 1)}
 
 
 def make_workload(rows, seed_batches=12):
