@@ -774,6 +774,47 @@ def main():
     raw_gbs = rrows * V * 8 / r0.elapsed_time(r1) / 1e6
     del raw
 
+    # ---- the same fetches from the condensed layout (compress_condensed's rows packed back
+    # to back with inclusive byte offsets): each row is read once, at its exact length
+    xw = x.numpy()
+    cond = torch.from_numpy(xw[np.arange(V)[None, :] < (sizes_np // 8)[:, None]]).pin_memory()
+    offs = torch.from_numpy(np.cumsum(sizes_np).astype(np.int64)).cuda()
+
+    def cond_step(k):
+        idx = batches_dev[k % len(batches_dev)]
+        _capi.check(lib.ibp_decompress_fetch_condensed(
+            cond.data_ptr(), cond.numel(), offs.data_ptr(), args.rows, V, 8, m.data_ptr(),
+            b.data_ptr(), idx.data_ptr(), idx.shape[0], out.data_ptr(), wsp.data_ptr(), wsb,
+            stream.cuda_stream))
+        return idx.shape[0]
+
+    for k in range(len(batches)):
+        n = cond_step(k)
+        torch.cuda.synchronize()
+        assert np.array_equal(out[:n].cpu().numpy(), d[batches[k]]), "condensed fetch mismatch"
+    for k in range(args.warmup):
+        cond_step(k)
+    torch.cuda.synchronize()
+    _capi.check(lib.ibp_profile_enable(args.steps))
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    crows = 0
+    for k in range(args.steps):
+        crows += cond_step(k)
+    c1.record()
+    c1.synchronize()
+    ckms = kernel_ms(args.steps)
+    cond_gbs = crows * V * 8 / c0.elapsed_time(c1) / 1e6
+    cond_fetch = sum(kuniq[:len(ckms)]) / sum(ckms) / 1e6
+    condensed = {"value": round(cond_gbs, 3), "unit": "GB/s",
+                 "kernel_achieved": round(cond_fetch, 3), "frac": round(cond_fetch / pcie, 4),
+                 "kernel_ms_per_launch": round(sum(ckms) / len(ckms), 4),
+                 "host_bytes": int(cond.numel() * 8),
+                 "what": "same batches from the condensed layout (exact-length row reads; "
+                         "ibp_decompress_fetch_condensed); kernel_achieved = compressed bytes "
+                         "of the distinct rows / fetch-kernel CUDA-event time"}
+    del cond, offs
+
     # ---- device-resident variant of the same fetch (HBM roofline)
     xd = x.cuda()
     hbm = None
@@ -848,6 +889,7 @@ def main():
                                         "what": "same batches, uncompressed pinned rows, "
                                                 "zero-copy gather (impl 2) with the same "
                                                 "sort and repeat fill"},
+            "condensed": condensed,
             "reference_gpu": ref_gpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),

@@ -168,6 +168,28 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                 int32_t nthreads, int32_t impl, void *workspace,
                                 size_t workspace_bytes, ibp_stream_t stream);
 
+/* ---------------------------------------------------------------- condensed fetch
+ * No counterpart in the reference, which writes the condensed layout (compress_condensed,
+ * src/compress.cu:238-313) but has no decompressor for it.  out row k = decompressed row
+ * index[k] (or k when num_index < 0) of `comp` (comp_words words), the condensed rows: row i
+ * occupies bytes
+ * [offsets[i-1], offsets[i]) (offsets[-1] = 0), i.e. the inclusive byte offsets that
+ * ibp_condensed_offsets produced; a row whose length is vec_size words is stored raw, any
+ * shorter one is compressed.  Each row is read once with its exact length (no fixed stride,
+ * no length guess).  offsets: num_vecs entries, device memory (pinned host works, slowly).
+ * Out-of-range indices set bit 0 of the status word; offsets that cannot describe a row of
+ * `comp` or a bitmap whose stream overruns its row set bit 1; those output rows are left
+ * untouched, and no read leaves the 16-byte blocks that hold `comp`.
+ * Workspace: ibp_decompress_fetch_workspace_size(num_index, vec_size, word_bytes,
+ * num_index >= 0). */
+ibp_status ibp_decompress_fetch_condensed(const void *comp, int64_t comp_words,
+                                          const int64_t *offsets, int64_t num_vecs,
+                                          int64_t vec_size, int word_bytes,
+                                          const void *mask, const void *bitval,
+                                          const int64_t *index, int64_t num_index, void *out,
+                                          void *workspace, size_t workspace_bytes,
+                                          ibp_stream_t stream);
+
 /* ---------------------------------------------------------------- batched multi-set fetch
  * No single counterpart in the reference, which fetches one tensor set per decompress_fetch
  * call (src/decompress.cu:10-156) and whose callers issue one call per table or tensor.  Here

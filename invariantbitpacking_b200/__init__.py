@@ -19,6 +19,7 @@ ibp_cuda.print_debug(False)
 
 __all__ = ["print_debug", "preprocess", "preprocess_kmeans", "get_compress_size",
            "get_single_compress_len", "compress_inplace", "compress", "compress_condensed",
+           "decompress_fetch_condensed",
            "decompress_fetch", "read_shared", "ibp_cuda", "IBPError"]
 
 
@@ -70,6 +71,13 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, device, comp_len=None,
                      index_arr=None, nblks=None, nthds=None, imp=None, output_tensor=None):
     return ibp_cuda.decompress_fetch(comp_dataset, mask, bitval, bitmask, device, comp_len,
                                      index_arr, nblks, nthds, imp, output_tensor)
+
+
+def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, device, index_arr=None,
+                               output_tensor=None):
+    """Rows of the condensed layout (compress_condensed's words and byte offsets)."""
+    return ibp_cuda.decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, device,
+                                               index_arr, output_tensor)
 
 
 def read_shared(filename, shape, dtype):

@@ -474,4 +474,46 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                      nthreads, impl, workspace, workspace_bytes, st);
 }
 
+// ------------------------------------------------------------------ condensed fetch
+ibp_status ibp_decompress_fetch_condensed(const void *comp, int64_t comp_words,
+                                          const int64_t *offsets, int64_t num_vecs,
+                                          int64_t vec_size, int word_bytes,
+                                          const void *mask, const void *bitval,
+                                          const int64_t *index, int64_t num_index, void *out,
+                                          void *workspace, size_t workspace_bytes,
+                                          ibp_stream_t stream) {
+    clear_error();
+    IBP_ARG(num_vecs >= 0 && vec_size >= 0 && comp_words >= 0,
+            "decompress_fetch_condensed: negative shape");
+    IBP_ARG(word_bytes == 4 || word_bytes == 8,
+            "decompress_fetch_condensed: Input tensor must be 4-byte or 8-byte datatype");
+    if (num_index < 0) index = nullptr;
+    const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
+    const bool work = nrows * vec_size > 0;
+    IBP_ARG(!work || (comp && offsets && mask && bitval),
+            "decompress_fetch_condensed: null rows/offsets/mask/bitval");
+    IBP_ARG(num_index <= 0 || index, "decompress_fetch_condensed: null index array");
+    IBP_ARG(out || !work, "decompress_fetch_condensed: null output");
+    if (work) {
+        IBP_ACCESSIBLE(comp, "decompress_fetch_condensed", "the condensed rows");
+        IBP_ACCESSIBLE(offsets, "decompress_fetch_condensed", "the offsets");
+        IBP_ACCESSIBLE(mask, "decompress_fetch_condensed", "mask");
+        IBP_ACCESSIBLE(bitval, "decompress_fetch_condensed", "bitval");
+        IBP_ACCESSIBLE(index, "decompress_fetch_condensed", "the index array");
+        IBP_ACCESSIBLE(out, "decompress_fetch_condensed", "the output");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (word_bytes == 4)
+        return decompress_impl<uint32_t>((const uint32_t *)comp, num_vecs, vec_size,
+                                         (const uint32_t *)mask, (const uint32_t *)bitval,
+                                         nullptr, index, num_index, num_index >= 0, -1,
+                                         (uint32_t *)out, -1, -1, -1, workspace,
+                                         workspace_bytes, st, offsets, comp_words * 4);
+    return decompress_impl<uint64_t>((const uint64_t *)comp, num_vecs, vec_size,
+                                     (const uint64_t *)mask, (const uint64_t *)bitval, nullptr,
+                                     index, num_index, num_index >= 0, -1, (uint64_t *)out, -1,
+                                     -1, -1, workspace, workspace_bytes, st, offsets,
+                                     comp_words * 8);
+}
+
 }  // extern "C"

@@ -49,7 +49,8 @@ struct FetchArgs {
 };
 
 // ------------------------------------------------------------------ fetch kernel
-template <typename U, int NC>
+// EXACT: condensed rows (byte ranges from a.s.offsets) instead of fixed-stride rows.
+template <typename U, int NC, bool EXACT>
 __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -76,10 +77,15 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         if (bad) atomicOr(a.status, kStatusBadIndex);
         head = head && !bad;
         U *orow = a.out + (head ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
-        const bool packed =
-            head && !a.raw_only && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1);
-        fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head, packed,
-                           a.status);
+        if constexpr (EXACT) {
+            fetch_heads_exact<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
+                                     a.status);
+        } else {
+            const bool packed =
+                head && !a.raw_only && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1);
+            fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head, packed,
+                               a.status);
+        }
     }
 }
 
@@ -138,7 +144,7 @@ size_t decompress_workspace(int64_t nidx, int64_t v, int wb, bool has_index) {
     return s.total();
 }
 
-template <typename U, int NC>
+template <typename U, int NC, bool EXACT>
 static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaStream_t st) {
     const size_t slot_bytes = (size_t)a.slot_words * sizeof(U);
     int threads = nthreads > 0 ? nthreads : kFetchThreads;
@@ -156,7 +162,7 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
         return IBP_ERR_UNSUPPORTED;
     }
     a.slots = slots;
-    auto kern = fetch_rows_kernel<U, NC>;
+    auto kern = fetch_rows_kernel<U, NC, EXACT>;
     IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int64_t blocks = nblks;
     if (blocks <= 0) {
@@ -176,20 +182,32 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     return IBP_OK;
 }
 
+template <typename U, bool EXACT>
+static ibp_status launch_fetch_x(FetchArgs<U> a, int nblks, int nthreads, cudaStream_t st) {
+    if (a.raw_only || a.s.v > 64) return launch_fetch_nc<U, 0, EXACT>(a, nblks, nthreads, st);
+    if (a.s.v > 32) return launch_fetch_nc<U, 2, EXACT>(a, nblks, nthreads, st);
+    return launch_fetch_nc<U, 1, EXACT>(a, nblks, nthreads, st);
+}
+
 template <typename U>
 static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStream_t st) {
     if (a.nrows <= 0) return IBP_OK;
-    a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, 16 / sizeof(U));
-    if (a.raw_only || a.s.v > 64) return launch_fetch_nc<U, 0>(a, nblks, nthreads, st);
-    if (a.s.v > 32) return launch_fetch_nc<U, 2>(a, nblks, nthreads, st);
-    return launch_fetch_nc<U, 1>(a, nblks, nthreads, st);
+    constexpr int per16 = 16 / sizeof(U);
+    if (a.s.offsets) {
+        // a condensed row starts at any word: room for the blocks around it and the padding
+        a.slot_words = (int64_t)align_up((size_t)a.s.v + 2 * per16 + 2, per16);
+        return launch_fetch_x<U, true>(a, nblks, nthreads, st);
+    }
+    a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, per16);
+    return launch_fetch_x<U, false>(a, nblks, nthreads, st);
 }
 
 template <typename U>
 ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                            const U *bitval, const int32_t *bitmask, const int64_t *idx,
                            int64_t nidx, bool has_index, int comp_len, U *out, int nblks,
-                           int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st) {
+                           int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st,
+                           const int64_t *offsets, int64_t comp_bytes) {
     const int wb = sizeof(U);
     const int64_t nrows = has_index ? nidx : n;
     const size_t need = decompress_workspace(nidx, v, wb, has_index);
@@ -213,6 +231,8 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     a.s.mw = meta_bytes(v, wb) / wb;
     a.s.t = t;
     a.s.bitmask = bitmask;
+    a.s.offsets = offsets;
+    a.s.comp_bytes = comp_bytes;
     a.s.first_words = first_read_words(v, a.s.mw, wb, comp_len);
     a.nrows = nrows;
     a.raw_only = impl == 2;
@@ -254,11 +274,11 @@ template ibp_status decompress_impl<uint32_t>(const uint32_t *, int64_t, int64_t
                                               const uint32_t *, const uint32_t *,
                                               const int32_t *, const int64_t *, int64_t, bool,
                                               int, uint32_t *, int, int, int, void *, size_t,
-                                              cudaStream_t);
+                                              cudaStream_t, const int64_t *, int64_t);
 template ibp_status decompress_impl<uint64_t>(const uint64_t *, int64_t, int64_t,
                                               const uint64_t *, const uint64_t *,
                                               const int32_t *, const int64_t *, int64_t, bool,
                                               int, uint64_t *, int, int, int, void *, size_t,
-                                              cudaStream_t);
+                                              cudaStream_t, const int64_t *, int64_t);
 
 }  // namespace ibp200

@@ -29,6 +29,8 @@ struct RowSet {
     int64_t first_words;    // words of the first read of a compressed row
     ColTables<U> t;         // per-column tables (device)
     const int32_t *bitmask; // compressed-row bits (device)
+    const int64_t *offsets; // condensed rows: inclusive end byte of each row (else nullptr)
+    int64_t comp_bytes;     // condensed rows: bytes of `comp`
 };
 
 // Copy row words [w0, w1) into the same positions of a shared slot: 16-byte loads when the
@@ -271,6 +273,107 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
                 // words past the stream read as zero (get_bits looks one word ahead; the
                 // value there never reaches an output bit)
                 if (lane < 2) buf[end[q] + lane] = 0;
+                __syncwarp();
+                decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
+                __syncwarp();
+            }
+        }
+    }
+}
+
+// Condensed rows (byte ranges known from the offsets): each head lane's row is read exactly,
+// its 16-byte blocks (at most 64 per row staged in registers, longer rows by a plain loop)
+// loaded for up to `nslots` rows before any is stored, so one round trip serves a row.  A
+// row whose stored length is the raw length is copied; any other is decoded, after checking
+// that its bitmap's stream fits the stored length.  Ranges that cannot be a row (negative,
+// decreasing, past the end of `comp`, longer than raw, not whole words) are flagged as
+// corrupt and skipped, so no read leaves the 16-byte blocks of `comp`.
+template <typename U, int NC>
+__device__ __forceinline__ void fetch_heads_exact(const RowSet<U> &s, const LaneTables<U, NC> &lt,
+                                                  U *__restrict__ slots, int nslots,
+                                                  int64_t slot_words, int64_t key, U *orow,
+                                                  bool head, int32_t *status) {
+    constexpr int per16 = 16 / sizeof(U);
+    const int lane = threadIdx.x & 31;
+    const int64_t v = s.v;
+    const int64_t raw_bytes = v * (int64_t)sizeof(U);
+    int64_t b0 = 0, b1 = 0;
+    if (head) {
+        b0 = key > 0 ? s.offsets[key - 1] : 0;
+        b1 = s.offsets[key];
+        if (b0 < 0 || b1 < b0 || b1 > s.comp_bytes || b1 - b0 > raw_bytes ||
+            ((b0 | b1) % (int64_t)sizeof(U)) != 0) {
+            atomicOr(status, kStatusCorruptRow);
+            head = false;
+        }
+    }
+    const char *base = reinterpret_cast<const char *>(s.comp);
+    unsigned hm = __ballot_sync(0xffffffffu, head);
+    while (hm) {
+        int lid[kRowsInFlight];
+        int cnt = 0;
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            lid[q] = 0;
+            if (q < nslots && hm) {
+                lid[q] = __ffs(hm) - 1;
+                hm &= hm - 1;
+                ++cnt;
+            }
+        }
+        int woff[kRowsInFlight];
+        {
+            uint4 stage[kRowsInFlight][2];
+            int64_t nblk[kRowsInFlight];
+#pragma unroll
+            for (int q = 0; q < kRowsInFlight; ++q) {
+                nblk[q] = 0;
+                woff[q] = 0;
+                if (q < cnt) {
+                    const int64_t lo = __shfl_sync(0xffffffffu, b0, lid[q]);
+                    const int64_t hi = __shfl_sync(0xffffffffu, b1, lid[q]);
+                    const uintptr_t a0 = (uintptr_t)(base + lo) & ~(uintptr_t)15;
+                    const uintptr_t a1 = ((uintptr_t)(base + hi) + 15) & ~(uintptr_t)15;
+                    woff[q] = (int)(((uintptr_t)(base + lo) - a0) / sizeof(U));
+                    const uint4 *src = reinterpret_cast<const uint4 *>(a0);
+                    const int64_t nb = (int64_t)((a1 - a0) >> 4);
+                    if (nb <= 64) {
+                        nblk[q] = nb;
+                        if (lane < nb) stage[q][0] = src[lane];
+                        if (lane + 32 < nb) stage[q][1] = src[lane + 32];
+                    } else {
+                        uint4 *dst = reinterpret_cast<uint4 *>(slots + q * slot_words);
+                        for (int64_t k = lane; k < nb; k += 32) dst[k] = src[k];
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kRowsInFlight; ++q) {
+                uint4 *dst = reinterpret_cast<uint4 *>(slots + q * slot_words);
+                if (lane < nblk[q]) dst[lane] = stage[q][0];
+                if (lane + 32 < nblk[q]) dst[lane + 32] = stage[q][1];
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            if (q < cnt) {
+                U *o = reinterpret_cast<U *>(
+                    __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
+                const int64_t len = (__shfl_sync(0xffffffffu, b1, lid[q]) -
+                                     __shfl_sync(0xffffffffu, b0, lid[q])) / (int64_t)sizeof(U);
+                U *buf = slots + q * slot_words + woff[q];
+                if (len == v) {
+                    for (int64_t j = lane; j < v; j += 32) o[j] = buf[j];
+                    __syncwarp();
+                    continue;
+                }
+                const int64_t end = row_words<U, NC>(buf, v, s.mw, s.t, lt);
+                if (end > len) {
+                    if (lane == 0) atomicOr(status, kStatusCorruptRow);
+                    continue;
+                }
+                if (lane < 2) buf[end + lane] = 0;
                 __syncwarp();
                 decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
                 __syncwarp();

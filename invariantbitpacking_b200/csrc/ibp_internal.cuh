@@ -54,7 +54,8 @@ template <typename U>
 ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                            const U *bitval, const int32_t *bitmask, const int64_t *idx,
                            int64_t nidx, bool has_index, int comp_len, U *out, int nblks,
-                           int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st);
+                           int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st,
+                           const int64_t *offsets = nullptr, int64_t comp_bytes = 0);
 
 // ---- k-means (ibp_kmeans.cu)
 size_t kmeans_workspace(int64_t n, int64_t v, int wb, int c);

@@ -309,6 +309,72 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
     return out
 
 
+def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, out_device,
+                               index_array_=None, output_tensor=None):
+    """Rows of the condensed layout written by compress_condensed (no reference
+    counterpart: the reference writes this layout but cannot read it back on the GPU).
+
+    comp: the condensed words (1-D, device or pinned host); offsets: the inclusive byte
+    offsets compress_condensed returned (int64, one per row; device, or pinned host).
+    Returns [len(index) or num_rows, vec_size] decompressed rows (non-blocking)."""
+    _torch_check(comp.device.type == "cuda" or comp.is_pinned(),
+                 "Input tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(comp.is_contiguous(), "Input tensor must be contiguous")
+    _torch_check(_gpu_accessible(offsets),
+                 "Offsets tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(offsets.dtype == torch.int64 and offsets.dim() == 1 and offsets.is_contiguous(),
+                 "Offsets tensor must be a contiguous 1D int64 tensor")
+    _torch_check(_gpu_accessible(mask),
+                 "Mask tensor must accessible by CUDA device (GPU or pinned memory)")
+    _torch_check(_gpu_accessible(bitval),
+                 "Bitval tensor must accessible by CUDA device (GPU or pinned memory)")
+    wb = comp.element_size()
+    _torch_check(wb in (4, 8), "Input tensor must be 4-byte or 8-byte datatype")
+    _torch_check(mask.element_size() == wb and bitval.element_size() == wb,
+                 "Mask and bitval tensors must have the same datatype size (4-byte or 8-byte) "
+                 "as input dataset")
+    v = int(vec_size)
+    _torch_check(mask.numel() >= v and bitval.numel() >= v,
+                 "Mask and bitval tensors must hold vec_size words")
+    n = offsets.shape[0]
+    out_device = torch.device(out_device)
+    if out_device.type == "cuda" and out_device.index is None:
+        out_device = torch.device("cuda", torch.cuda.current_device())
+    idx = None
+    if index_array_ is not None:
+        _torch_check(index_array_.device.type == "cuda",
+                     "Index array must accessible by CUDA device (GPU or pinned memory)")
+        _torch_check(index_array_.dim() == 1, "Index array should be 1D")
+        idx = index_array_.to(torch.int64).contiguous()
+    nrows = n if idx is None else idx.shape[0]
+    if output_tensor is not None:
+        _torch_check(output_tensor.device == out_device,
+                     "Output tensor device does not match specified output device")
+        _torch_check(output_tensor.dtype == comp.dtype,
+                     "Output tensor dtype does not match input dataset dtype")
+        _torch_check(output_tensor.shape[0] == nrows and output_tensor.shape[1] == v,
+                     "Output tensor shape does not match expected decompressed shape")
+        out = output_tensor
+    else:
+        out = torch.empty((nrows, v), dtype=comp.dtype, device=out_device)
+    if out_device.type != "cuda" and not out.is_pinned():
+        out = out.pin_memory()
+    dev = _cuda_device(comp, mask, idx, out)
+    with torch.cuda.device(dev):
+        need = _lib.ibp_decompress_fetch_workspace_size(nrows, v, wb, 0 if idx is None else 1)
+        ws, wsb = _workspace(need, dev)
+        _check(_lib.ibp_decompress_fetch_condensed(
+            _ptr(comp), comp.numel(), _ptr(offsets), n, v, wb, _ptr(mask), _ptr(bitval), _ptr(idx),
+            -1 if idx is None else nrows, _ptr(out), _ptr(ws), wsb, _stream()))
+        if _debug and ws is not None:
+            st = torch.zeros(1, dtype=torch.int32)
+            import ctypes
+            _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), _stream()))
+            if int(st[0]) & 3:
+                print("[ibp] decompress_fetch_condensed: bad index or corrupt row; skipped")
+    return out
+
+
 def read_shared(filename, shape, dtype):
     """src/ibp_api.cu:52-122: file contents in a new shared-memory CPU tensor."""
     t = torch.empty(list(shape), dtype=dtype).share_memory_()
