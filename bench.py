@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--config", default="graph_features",
                     choices=["graph_features", "embedding_tables", "decoder_layer",
-                             "served_mix"])
+                             "served_mix", "embedding_bag"])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=300)
     ap.add_argument("--batch-mb", type=int, default=128,
@@ -470,6 +470,83 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_embedding_bag(args):
+    """The DLRM caller (ColossalAI CachedEmbeddingBag with IBP, tests/dlrm_comp_merged.py):
+    the 26 embedding tables merged into one host-resident table with a GPU cache of 1% of
+    its rows; a step looks up 2048 uniformly drawn rows of every table (bags of one row, as
+    the reference's harness draws them) through the cached embedding bag, compressed
+    (comp=True) against the same bag over the raw table (comp=False, an all-zero bitmask: a
+    zero-copy gather), both fetched by this engine."""
+    import torch
+    torch.cuda.set_device(0)
+    from invariantbitpacking_b200 import synthetic, _capi
+    from invariantbitpacking_b200.callers import CompressedEmbeddingBag
+    lib = _capi.lib
+    tables = synthetic.embedding_tables()
+    starts = np.concatenate([[0], np.cumsum([t.shape[0] for t in tables])[:-1]])
+    merged = torch.from_numpy(np.concatenate(tables).view(np.float32))
+    rows, dim = merged.shape
+    del tables
+    sizes = np.diff(np.concatenate([starts, [rows]]))
+    per = 2048
+    rng = np.random.default_rng(200)
+    batches = []
+    for _ in range(64):
+        idx = np.concatenate([starts[i] + rng.integers(0, sizes[i], per)
+                              for i in range(len(sizes))])
+        batches.append(torch.from_numpy(idx).cuda())
+    offsets = torch.arange(per * len(sizes), device="cuda")
+    res = {}
+    for comp in (True, False):
+        t0 = time.perf_counter()
+        bag = CompressedEmbeddingBag(rows, dim, cache_ratio=0.01, _weight=merged, comp=comp)
+        setup = time.perf_counter() - t0
+        full_check = merged[batches[0].cpu()].cuda()
+        got = bag(batches[0], offsets)
+        torch.cuda.synchronize()
+        assert torch.equal(got, full_check), "embedding bag mismatch"
+        for k in range(args.warmup):
+            bag(batches[k % len(batches)], offsets)
+        torch.cuda.synchronize()
+        for key in bag.stats:
+            bag.stats[key] = 0
+        l0 = lib.ibp_kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(args.steps):
+            bag(batches[k % len(batches)], offsets)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = dict(bag.stats)
+        res[comp] = {"ms_per_step": round(ms / args.steps, 4),
+                     "lookups_per_s": round(st["lookups"] / ms * 1e3, 1),
+                     "fetched_GBps": round(st["fetched_bytes"] / ms / 1e6, 3),
+                     "hit_rate": round(st["hits"] / max(st["lookups"], 1), 4),
+                     "setup_s": round(setup, 2),
+                     "launches": int(lib.ibp_kernel_launch_count() - l0)}
+        if comp:
+            res["compressed_fraction"] = round(
+                float(bag.comp_len) / bag.words, 4) if bag.comp_len else None
+        del bag
+        torch.cuda.empty_cache()
+    line = {
+        "metric": "cached embedding bag over a host-resident table: distinct rows fetched per "
+                  "second into the GPU cache (GB/s), compressed vs raw",
+        "value": res[True]["fetched_GBps"], "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": res[True]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "embedding_bag: 26 tables merged, "
+                               f"{rows} x {dim} fp32 pinned host, GPU cache 1% of rows, "
+                               f"{per} uniform lookups per table per step, bags of one row",
+                   "compressed_len_fraction": res.get("compressed_fraction")},
+        "compressed": res[True], "raw": res[False],
+        "gpu_launches": res[True]["launches"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def served_sets(torch, ibp):
     """8 host-pinned sets from the plain/graph/embedding generators, rows re-shaped to
     V in {64, 128, 256, 512} int64 words, ~384 MB each."""
@@ -640,6 +717,13 @@ def main():
                               "compares against per-request fetches in the same line"}))
             return
         run_served(args)
+        return
+    if args.config == "embedding_bag":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the embedding-bag "
+                              "configuration compares compressed and raw tables in one line"}))
+            return
+        run_embedding_bag(args)
         return
     if args.config != "graph_features":
         if args.impl == "reference":
