@@ -71,3 +71,19 @@ def test_compressed_embedding_bag_matches_full_table(callers, comp):
     st = bag.stats
     assert st["misses"] > 0 and st["hits"] > 0
     assert st["lookups"] == st["hits"] + st["misses"]
+
+
+def test_sharded_fetcher_single_rank(callers):
+    import invariantbitpacking_b200 as ibp
+    from invariantbitpacking_b200.shard import ShardedFetcher
+    rng = np.random.default_rng(2)
+    f = rng.normal(0, 0.5, (5000, 64)).astype(np.float32)
+    d = (f.view(np.uint32) & np.uint32(0xFFFF0000)).view(np.int64)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    bm = ibp.compress_inplace(x, m, b)
+    sf = ShardedFetcher(x, m, b, bm, ibp.get_single_compress_len(x, m, b))
+    idx = torch.from_numpy(rng.integers(0, 5000, 777))
+    rows, (lo, hi) = sf(idx)
+    assert (lo, hi) == (0, 777) and np.array_equal(rows.cpu().numpy(), d[idx.numpy()])
+    assert np.array_equal(sf(idx, gather=True).cpu().numpy(), d[idx.numpy()])
