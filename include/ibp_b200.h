@@ -55,6 +55,13 @@ int ibp_abi_version(void);
 /* Debug prints to stdout; replaces print_debug (src/ibp_api.cu:7-12). */
 void ibp_set_debug(int on);
 
+/* How decompress_fetch (and its condensed and no-alloc forms) finds the repeated rows of an
+ * index array, process-wide: 0 = auto (hash table for fixed-stride compressed rows when the
+ * index has fewer than a quarter as many entries as the set has rows, else sort), 1 = always
+ * sort (rows then fetched in row order), 2 = always hash.  No counterpart in the reference
+ * (it always sorts). */
+ibp_status ibp_set_fetch_dedup(int32_t mode);
+
 /* Profiling hooks (benchmarks): after ibp_profile_enable(cap), the next `cap` row-fetch
  * kernel launches (decompress_fetch, any thread) are bracketed by CUDA events on their
  * stream.  ibp_profile_take waits for them, writes their durations in milliseconds to ms[]
@@ -298,8 +305,8 @@ ibp_status ibp_server_destroy(ibp_server *srv);
  * ibp_decompress_fetch without nblks/nthreads/impl/workspace; its scratch is a static 4 MiB
  * (4194304-byte) device array that the library reserves on every device that loads it, until
  * the process exits.  A call that needs more scratch than that
- * (ibp_decompress_fetch_workspace_size(...) > 4194304; roughly: more than ~50k index entries
- * of 8-byte words) returns IBP_ERR_WORKSPACE before launching anything.  The first call on a
+ * (ibp_decompress_fetch_workspace_size(...) > 4194304; roughly: more than ~130k index
+ * entries) returns IBP_ERR_WORKSPACE before launching anything.  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress, with that device
  * current): make that first call before any stream capture on the device.  All calls share
  * the array, and calls whose GPU work overlaps (other streams, other threads) race on it:

@@ -28,6 +28,7 @@ SIGNATURES = {
     "ibp_abi_version": (_INT, []),
     "ibp_set_debug": (None, [_INT]),
     "ibp_read_status": (_INT, [_P, _P, _P]),
+    "ibp_set_fetch_dedup": (_INT, [_I32]),
     "ibp_profile_enable": (_INT, [_I32]),
     "ibp_profile_take": (_I32, [_P, _I32]),
     "ibp_kernel_launch_count": (ctypes.c_ulonglong, []),

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -27,6 +28,9 @@ static Profiler &profiler() {
     static Profiler p;
     return p;
 }
+
+static std::atomic<int> g_dedup_mode{0};
+int fetch_dedup_mode() { return g_dedup_mode.load(std::memory_order_relaxed); }
 
 int profile_begin(cudaStream_t st) {
     Profiler &p = profiler();
@@ -166,6 +170,13 @@ const char *ibp_last_error(void) { return g_err.c_str(); }
 int ibp_abi_version(void) { return 1; }
 
 void ibp_set_debug(int on) { g_debug = on != 0; }
+
+ibp_status ibp_set_fetch_dedup(int32_t mode) {
+    clear_error();
+    IBP_ARG(mode >= 0 && mode <= 2, "set_fetch_dedup: mode must be 0 (auto), 1 (sort) or 2 (hash)");
+    g_dedup_mode.store(mode);
+    return IBP_OK;
+}
 
 ibp_status ibp_profile_enable(int32_t capacity) {
     clear_error();

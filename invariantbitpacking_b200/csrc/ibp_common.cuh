@@ -22,6 +22,7 @@ extern std::atomic<unsigned long long> g_launches;  // engine kernels launched s
 // Optional CUDA events around row-fetch kernel launches (benchmark profiling hook):
 // profile_begin returns a slot (or -1 when profiling is off or full), profile_end closes it.
 int profile_begin(cudaStream_t st);
+int fetch_dedup_mode();  // ibp_set_fetch_dedup: 0 auto, 1 sort, 2 hash
 void profile_end(int slot, cudaStream_t st);
 
 #define IBP_DPRINTF(...)                       \

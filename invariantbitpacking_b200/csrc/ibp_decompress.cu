@@ -16,13 +16,17 @@
 //    them at the non-invariant positions (log2(W) branch-free steps).  For rows of up to 64
 //    words the per-column tables (mask, bitval, kept bits, move masks) live in registers,
 //    loaded once per warp; longer rows read them through the L1 cache.
-//  * index arrays: rows are fetched in sorted index order (cub radix sort on only the bits
-//    the row count needs) so concurrent warps read neighbouring host pages, and each
-//    distinct row crosses PCIe once; repeats are filled afterwards by a copy kernel that
-//    reads each source row once per 32 positions (Zipf mini-batches repeat hot rows a lot).
+//  * index arrays: each distinct row crosses PCIe once.  Dense batches (a quarter of the
+//    rows or more), condensed rows and raw gathers are fetched in sorted index order (cub
+//    radix sort on only the bits the row count needs) so concurrent warps read neighbouring
+//    host pages; sparse batches of fixed-stride compressed rows, where order gains little,
+//    claim rows in an open-addressing hash table instead of sorting.  Repeats are filled
+//    afterwards by a copy kernel (Zipf mini-batches repeat hot rows a lot).
 //  * no allocation, no host synchronisation: everything lives in the caller's workspace
 //    and is enqueued on the caller's stream.
 #include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
 
 #include "ibp_codec.cuh"
 #include "ibp_fetch.cuh"
@@ -45,8 +49,80 @@ struct FetchArgs {
     unsigned long long *work;  // chunk counter, zero at launch
     int64_t slot_words;   // shared-memory words per row slot
     int slots;            // row slots per warp (<= kRowsInFlight)
-    int upos;             // positions per chunk (unit_positions: 4..32)
+    int upos;             // positions per chunk the grid was sized for (unit_positions)
+    int64_t *hkeys;       // hashed dedup: open-addressing table of rows (-1 = empty) ...
+    int64_t *hpos;        // ... and the position that claimed each (nullptr: no table)
+    int64_t hslots;       // the table's slots
 };
+
+// ------------------------------------------------------------------ hashed dedup
+// The first position to claim a row in the table fetches it; later ones are repeats.  The
+// table has at least twice as many slots as positions, so linear probing ends quickly.
+__device__ __forceinline__ uint64_t row_hash(int64_t key, int64_t slots) {
+    return __umul64hi((uint64_t)key * 0x9E3779B97F4A7C15ull, (uint64_t)slots);
+}
+
+__device__ __forceinline__ bool hash_claim(int64_t *keys, int64_t *pos, int64_t slots,
+                                           int64_t key, int64_t k) {
+    uint64_t h = row_hash(key, slots);
+    for (int64_t probe = 0; probe < slots; ++probe) {
+        const unsigned long long old = atomicCAS(
+            reinterpret_cast<unsigned long long *>(keys + h), ~0ull, (unsigned long long)key);
+        if (old == ~0ull) {
+            pos[h] = k;
+            return true;
+        }
+        if ((int64_t)old == key) return false;
+        h = h + 1 == (uint64_t)slots ? 0 : h + 1;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
+                                             const int64_t *__restrict__ pos, int64_t slots,
+                                             int64_t key) {
+    uint64_t h = row_hash(key, slots);
+    for (int64_t probe = 0; probe < slots; ++probe) {
+        const int64_t kk = keys[h];
+        if (kk == key) return pos[h];
+        if (kk == -1) return -1;
+        h = h + 1 == (uint64_t)slots ? 0 : h + 1;
+    }
+    return -1;
+}
+
+// Repeats of a hashed fetch: each position whose row another position claimed copies that
+// position's output row (a warp per row copy, 16-byte moves when both rows are aligned).
+template <typename U>
+__global__ void __launch_bounds__(256)
+fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
+                   const int64_t *__restrict__ hkeys, const int64_t *__restrict__ hpos,
+                   int64_t hslots, U *__restrict__ out, int64_t v) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t bytes = v * (int64_t)sizeof(U);
+    for (int64_t k0 = warp * 32; k0 < nrows; k0 += nwarps * 32) {
+        const int64_t k = k0 + lane;
+        const int64_t key = k < nrows ? idx[k] : -1;
+        int64_t hp = -1;
+        if (key >= 0 && key < n) hp = hash_find(hkeys, hpos, hslots, key);
+        unsigned dm = __ballot_sync(0xffffffffu, hp >= 0 && hp != k);
+        while (dm) {
+            const int j = __ffs(dm) - 1;
+            dm &= dm - 1;
+            const U *src = out + __shfl_sync(0xffffffffu, hp, j) * v;
+            U *dst = out + (k0 + j) * v;
+            if (((((uintptr_t)src) | ((uintptr_t)dst)) & 15) == 0 && (bytes & 15) == 0) {
+                const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+                uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+                for (int64_t q = lane; q < bytes / 16; q += 32) d4[q] = s4[q];
+            } else {
+                for (int64_t q = lane; q < v; q += 32) dst[q] = src[q];
+            }
+        }
+    }
+}
 
 // ------------------------------------------------------------------ fetch kernel
 // EXACT: condensed rows (byte ranges from a.s.offsets) instead of fixed-stride rows.
@@ -57,15 +133,21 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
     U *slots = reinterpret_cast<U *>(smem) + (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
     LaneTables<U, NC> lt;
     if (!a.raw_only) lt.load(a.s.t, a.s.v);
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    int64_t seen = 0;  // positions handed out when this warp last took a chunk
     for (;;) {
-        unsigned long long chunk = 0;
-        if (lane == 0) chunk = atomicAdd(a.work, 1ull);
-        chunk = __shfl_sync(0xffffffffu, chunk, 0);
-        const int64_t k0 = (int64_t)chunk * a.upos;
+        // guided self-scheduling: 32-position chunks while much work remains, shrinking to
+        // 4 towards the end, so that the grid's last chunks (each a chain of dependent
+        // reads) finish close together
+        const int g = (int)min((int64_t)32, max((int64_t)4, (a.nrows - seen) / (2 * nwarps)));
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(a.work, (unsigned long long)g);
+        const int64_t k0 = (int64_t)__shfl_sync(0xffffffffu, c, 0);
         if (k0 >= a.nrows) break;
+        seen = k0 + g;
         // lane-parallel metadata of the chunk's positions
         const int64_t k = k0 + lane;
-        const bool valid = lane < a.upos && k < a.nrows;
+        const bool valid = lane < g && k < a.nrows;
         const int64_t key = valid ? (a.keys ? a.keys[k] : k) : -1;
         bool head = valid;
         if (a.dedup) {
@@ -76,6 +158,7 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         const bool bad = head && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         head = head && !bad;
+        if (a.hkeys && head) head = hash_claim(a.hkeys, a.hpos, a.hslots, key, k);
         U *orow = a.out + (head ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
         if constexpr (EXACT) {
             fetch_heads_exact<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
@@ -130,16 +213,25 @@ static size_t sort_temp_bytes(int64_t nidx) {
     return temp;
 }
 
+// Slots of the hashed dedup table for nidx positions (load factor at most one half).
+static int64_t hash_slots(int64_t nidx) { return std::max<int64_t>(64, (2 * nidx + 63) / 64 * 64); }
+
 size_t decompress_workspace(int64_t nidx, int64_t v, int wb, bool has_index) {
     Sizer s;
     s.take<char>(kStatusBytes);
     s.take<char>(wb == 8 ? tables_bytes<uint64_t>(v) : tables_bytes<uint32_t>(v));
     if (has_index && nidx > 0) {
-        s.take<int64_t>(nidx);  // iota
-        s.take<int64_t>(nidx);  // sanitised keys
-        s.take<int64_t>(nidx);  // sorted keys
-        s.take<int64_t>(nidx);  // positions
-        s.take<char>(sort_temp_bytes(nidx));
+        // either the sort's arrays or the hash table, whichever the call picks
+        Sizer srt;
+        srt.take<int64_t>(nidx);  // iota
+        srt.take<int64_t>(nidx);  // sanitised keys
+        srt.take<int64_t>(nidx);  // sorted keys
+        srt.take<int64_t>(nidx);  // positions
+        srt.take<char>(sort_temp_bytes(nidx));
+        Sizer hsh;
+        hsh.take<int64_t>(hash_slots(nidx));
+        hsh.take<int64_t>(hash_slots(nidx));
+        s.take<char>(std::max(srt.total(), hsh.total()));
     }
     return s.total();
 }
@@ -244,6 +336,26 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     if (nidx > 0x7fffffffLL) {
         set_error("decompress_fetch: index arrays above 2^31-1 entries are not supported");
         return IBP_ERR_UNSUPPORTED;
+    }
+    const int mode = fetch_dedup_mode();
+    if (mode == 2 || (mode == 0 && 4 * nidx < n && !offsets && impl != 2)) {
+        // sparse batch of fixed-stride compressed rows: claim rows in a hash table instead
+        // of sorting (row order gains little when the rows are far apart; condensed and
+        // raw rows do lose without it, so they keep the sort)
+        const int64_t slots = hash_slots(nidx);
+        int64_t *hkeys = c.take<int64_t>(slots);
+        int64_t *hpos = c.take<int64_t>(slots);
+        IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, sizeof(int64_t) * slots, st));
+        a.keys = idx;
+        a.hkeys = hkeys;
+        a.hpos = hpos;
+        a.hslots = slots;
+        IBP_RET(launch_fetch<U>(a, nblks, nthreads, st));
+        const int64_t fb = std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
+        fill_hashed_kernel<U><<<(unsigned)fb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
+                                                            out, v);
+        IBP_LAUNCHED("fill_hashed_kernel");
+        return IBP_OK;
     }
     int64_t *iota = c.take<int64_t>(nidx);
     int64_t *keys_in = c.take<int64_t>(nidx);

@@ -1,0 +1,76 @@
+"""Both ways decompress_fetch finds repeated rows -- radix sort, and the open-addressing hash
+table it uses for sparse batches -- must give the oracle's rows bit for bit: repeats, hot
+rows, out-of-range entries, empty and single-entry indices, 4- and 8-byte words, row
+lengths that break 16-byte alignment, host and device sets, and the condensed layout."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ibp():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import invariantbitpacking_b200 as m
+    return m
+
+
+@pytest.fixture(params=[1, 2, 0], ids=["sort", "hash", "auto"])
+def mode(request, ibp):
+    from invariantbitpacking_b200 import _capi
+    _capi.check(_capi.lib.ibp_set_fetch_dedup(request.param))
+    yield request.param
+    _capi.check(_capi.lib.ibp_set_fetch_dedup(0))
+
+
+def make(rng, n, v, wb):
+    f = rng.normal(0, 0.4, (n, v * wb // 4)).astype(np.float32)
+    f = (f.view(np.uint32) & np.uint32(0xFFFF8000)).view(np.float32)
+    return np.ascontiguousarray(f).view(np.int64 if wb == 8 else np.int32)
+
+
+@pytest.mark.parametrize("wb,v", [(8, 64), (8, 7), (4, 33), (4, 128), (8, 300)])
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_dedup_modes_match_oracle(ibp, oracle, mode, wb, v, where):
+    rng = np.random.default_rng(v * 10 + wb)
+    n = 20000
+    d = make(rng, n, v, wb)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    bm = ibp.compress_inplace(x, m, b)
+    cl = ibp.get_single_compress_len(x, m, b)
+    if where == "device":
+        x = x.cuda()
+    comp = x.cpu().numpy()
+    cases = [
+        rng.integers(0, n, 3000),                         # sparse, some repeats
+        np.repeat(rng.integers(0, n, 50), 40),            # few rows, long runs
+        rng.integers(0, n, 40000),                        # denser than the set
+        np.array([n - 1]), np.array([], dtype=np.int64),
+        np.concatenate([rng.integers(0, n, 500), [-1, n, 10 ** 12, 5, 5]]),
+    ]
+    for idx in cases:
+        ti = torch.from_numpy(idx.astype(np.int64)).cuda()
+        out = torch.full((idx.size, v), 7, dtype=x.dtype, device="cuda")
+        ibp.decompress_fetch(x, m, b, bm, "cuda", cl, ti, output_tensor=out)
+        got = out.cpu().numpy()
+        ok = (idx >= 0) & (idx < n)
+        want = oracle.decompress(comp, m.cpu().numpy(), b.cpu().numpy(), bm.cpu().numpy(),
+                                 np.where(ok, idx, 0))
+        assert np.array_equal(got[ok], want[ok])
+        assert (got[~ok] == 7).all()   # skipped rows are left untouched
+
+
+def test_dedup_modes_condensed(ibp, mode):
+    rng = np.random.default_rng(5)
+    n, v = 9000, 40
+    d = make(rng, n, v, 8)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    comp, offs = ibp.compress_condensed(x, m, b)
+    for idx in (rng.integers(0, n, 1500), np.repeat(rng.integers(0, n, 30), 17)):
+        out = ibp.decompress_fetch_condensed(comp, offs.cuda(), m, b, v, "cuda",
+                                             torch.from_numpy(idx).cuda())
+        assert np.array_equal(out.cpu().numpy(), d[idx])
