@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--config", default="graph_features",
                     choices=["graph_features", "embedding_tables", "decoder_layer",
-                             "served_mix", "embedding_bag"])
+                             "served_mix", "embedding_bag", "device_rows"])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=300)
     ap.add_argument("--shard", action="store_true",
@@ -550,6 +550,111 @@ def run_embedding_bag(args):
     print(json.dumps(line), flush=True)
 
 
+def run_device_rows(args):
+    """The reference's device-resident decompression benchmark (tests/dev_decomp_thput.py):
+    100,000 int32 rows of 256, 1024 and 4096 bytes (all zeros) compressed in HBM under
+    random masks that make a target share of the bits invariant (12.5% .. 97%), decompressed
+    whole (no index).  Our decompress_fetch against the reference's own (built from its
+    sources for sm_100a, its script's 320 blocks x 512 threads, impls 0 and 1) and a plain
+    clone of the uncompressed rows; CUDA-event times, bit-exact checks on every output."""
+    import glob
+    import torch
+    torch.cuda.set_device(0)
+    import invariantbitpacking_b200 as ibp
+    from invariantbitpacking_b200 import _capi
+    lib = _capi.lib
+    ref = None
+    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    if mods:
+        sys.path.insert(0, os.path.dirname(mods[0]))
+        import ibp_cuda as ref
+        ref.print_debug(False)
+    num = 100_000
+    rng = np.random.default_rng(11)
+    reps = max(3, min(args.steps, 20))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    points, launches = [], 0
+    with Clocks(torch.cuda.current_device()) as clk:
+        for size in (256, 1024, 4096):
+            v = size // 4
+            t = torch.zeros((num, v), dtype=torch.int32, device="cuda")
+            clone_ms = timed(lambda: t.clone())
+            for rate in (0.125, 0.25, 0.5, 0.75, 0.9, 0.95, 0.97):
+                # mask bits drawn at random until rate x row bits (+ V + 1) are set; bitval
+                # row 0 (zeros), as the reference script makes them
+                bits = 32 * v
+                sel = rng.permutation(bits)[:min(bits, int(rate * bits) + v + 1)]
+                mw = np.zeros(v, np.uint32)
+                np.bitwise_or.at(mw, sel // 32, np.uint32(1) << (sel % 32).astype(np.uint32))
+                mask = torch.from_numpy(mw.view(np.int32)).cuda()
+                bitval = torch.zeros(v, dtype=torch.int32, device="cuda")
+                x = t.clone()
+                comp_frac = float(ibp.get_compress_size(x, mask, bitval).sum()) / (num * size)
+                bm = ibp.compress_inplace(x, mask, bitval)
+                cl = ibp.get_single_compress_len(x, mask, bitval)
+                out = torch.empty_like(t)
+                l0 = lib.ibp_kernel_launch_count()
+                ours = timed(lambda: ibp.decompress_fetch(x, mask, bitval, bm, "cuda", cl, None,
+                                                          output_tensor=out))
+                launches += lib.ibp_kernel_launch_count() - l0
+                assert torch.equal(out, t), "device-rows mismatch"
+                pt = {"row_bytes": size, "invariant_target": rate,
+                      "compressed_fraction": round(comp_frac, 4),
+                      "ours_us": round(ours * 1e3, 1), "clone_us": round(clone_ms * 1e3, 1),
+                      "ours_GBps": round(num * size / ours / 1e6, 1)}
+                if ref is not None:
+                    for impl in (0, 1):
+                        xr = t.clone()
+                        bmr = ref.compress_inplace(xr, mask, bitval, None)
+                        holder = {}
+
+                        def rcall():
+                            holder["o"] = ref.decompress_fetch(xr, mask, bitval, bmr,
+                                                               torch.device("cuda"), cl, None,
+                                                               320, 512, impl, None)
+                        rt = timed(rcall)
+                        pt[f"ref_impl{impl}_us"] = round(rt * 1e3, 1)
+                        pt[f"ref_impl{impl}_exact"] = bool(torch.equal(holder["o"], t))
+                    pt["speedup_vs_ref_impl0"] = round(pt["ref_impl0_us"] / pt["ours_us"], 2)
+                points.append(pt)
+                del x, out
+            del t
+            torch.cuda.empty_cache()
+    head = [p for p in points if p["row_bytes"] == 1024 and p["invariant_target"] == 0.5][0]
+    sp = [p["speedup_vs_ref_impl0"] for p in points if "speedup_vs_ref_impl0" in p]
+    line = {
+        "metric": "device-resident decompress delivered GB/s (100k rows in HBM, no index; "
+                  "reference dev_decomp_thput pattern)",
+        "value": head["ours_GBps"], "unit": "GB/s", "n_gpus": 1, "steps": reps,
+        "warmup": args.warmup, "ms_per_step": round(head["ours_us"] / 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": "device_rows: 100,000 zero int32 rows of 256/1024/4096 B in HBM, "
+                               "random masks at 7 invariant-bit targets; line value = 1024 B "
+                               "rows at 50%", "l2": "outputs 25-410 MB; 1024/4096 B sets "
+                                                   "exceed L2"},
+        "speedup_vs_ref_impl0": {"min": min(sp) if sp else None,
+                                 "geomean": round(float(np.exp(np.mean(np.log(sp)))), 2)
+                                 if sp else None, "max": max(sp) if sp else None},
+        "points": points,
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def served_sets(torch, ibp):
     """8 host-pinned sets from the plain/graph/embedding generators, rows re-shaped to
     V in {64, 128, 256, 512} int64 words, ~384 MB each."""
@@ -720,6 +825,13 @@ def main():
                               "compares against per-request fetches in the same line"}))
             return
         run_served(args)
+        return
+    if args.config == "device_rows":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the device-rows "
+                              "configuration times the reference's GPU build in the same line"}))
+            return
+        run_device_rows(args)
         return
     if args.config == "embedding_bag":
         if args.impl == "reference":

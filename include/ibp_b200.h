@@ -56,8 +56,9 @@ int ibp_abi_version(void);
 void ibp_set_debug(int on);
 
 /* How decompress_fetch (and its condensed and no-alloc forms) finds the repeated rows of an
- * index array, process-wide: 0 = auto (hash table for fixed-stride compressed rows when the
- * index has fewer than a quarter as many entries as the set has rows, else sort), 1 = always
+ * index array, process-wide: 0 = auto (hash table for fixed-stride compressed rows in device
+ * memory, or in host memory when the index has fewer than a quarter as many entries as the
+ * set has rows; else sort), 1 = always
  * sort (rows then fetched in row order), 2 = always hash.  No counterpart in the reference
  * (it always sorts). */
 ibp_status ibp_set_fetch_dedup(int32_t mode);

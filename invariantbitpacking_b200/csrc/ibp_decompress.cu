@@ -16,11 +16,12 @@
 //    them at the non-invariant positions (log2(W) branch-free steps).  For rows of up to 64
 //    words the per-column tables (mask, bitval, kept bits, move masks) live in registers,
 //    loaded once per warp; longer rows read them through the L1 cache.
-//  * index arrays: each distinct row crosses PCIe once.  Dense batches (a quarter of the
-//    rows or more), condensed rows and raw gathers are fetched in sorted index order (cub
-//    radix sort on only the bits the row count needs) so concurrent warps read neighbouring
-//    host pages; sparse batches of fixed-stride compressed rows, where order gains little,
-//    claim rows in an open-addressing hash table instead of sorting.  Repeats are filled
+//  * index arrays: each distinct row crosses PCIe once.  Dense batches of host rows (a
+//    quarter of the rows or more), condensed rows and raw gathers are fetched in sorted
+//    index order (cub radix sort on only the bits the row count needs) so concurrent warps
+//    read neighbouring host pages; fixed-stride compressed rows in HBM, and sparse batches of
+//    them in host memory, where order gains little, claim rows in an open-addressing hash
+//    table instead of sorting.  Repeats are filled
 //    afterwards by a copy kernel (Zipf mini-batches repeat hot rows a lot).
 //  * no allocation, no host synchronisation: everything lives in the caller's workspace
 //    and is enqueued on the caller's stream.
@@ -338,10 +339,19 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         return IBP_ERR_UNSUPPORTED;
     }
     const int mode = fetch_dedup_mode();
-    if (mode == 2 || (mode == 0 && 4 * nidx < n && !offsets && impl != 2)) {
-        // sparse batch of fixed-stride compressed rows: claim rows in a hash table instead
-        // of sorting (row order gains little when the rows are far apart; condensed and
-        // raw rows do lose without it, so they keep the sort)
+    bool on_device = false;
+    {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, comp) == cudaSuccess)
+            on_device = pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged;
+        else
+            cudaGetLastError();
+    }
+    if (mode == 2 || (mode == 0 && !offsets && impl != 2 && (on_device || 4 * nidx < n))) {
+        // fixed-stride compressed rows in HBM, or a sparse batch of them in host memory:
+        // claim rows in a hash table instead of sorting (HBM does not care about row order,
+        // and far-apart host rows gain little from it; condensed and raw rows and dense host
+        // batches do lose without it, so they keep the sort)
         const int64_t slots = hash_slots(nidx);
         int64_t *hkeys = c.take<int64_t>(slots);
         int64_t *hpos = c.take<int64_t>(slots);

@@ -86,7 +86,12 @@ __device__ __forceinline__ U scatter_regs(U y, U sel, const U *mv) {
 }
 
 // Decode one compressed row from its shared-memory slot (bitmap at word 0, stream at word
-// mw, zero words after the stream) into the output row.
+// mw, zero words after the stream) into the output row.  Lane j of a 32-word chunk takes
+// its bit length (kept bits when compressible, W otherwise) and its stream offset, pulls its
+// bits with a funnel read and scatters them to the column's non-invariant positions; a warp
+// prefix sum per chunk of 32 columns gives the offsets.  Rows of up to 64 words use the
+// lane's register tables, one chunk after the other; longer rows take their chunks four at
+// a time with the prefix sums interleaved, so different chunks' shuffle chains overlap.
 template <typename U, int NC>
 __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v, int64_t mw,
                                            const ColTables<U> &t, const LaneTables<U, NC> &lt,
@@ -95,41 +100,65 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
     const int lane = threadIdx.x & 31;
     const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
     const U *stream = buf + mw;
-    int64_t base = 0;
-    auto chunk = [&](int64_t c0, U m, U bv, int nbits, const U *mv, int stride) {
-        const int64_t j = c0 + lane;
-        const bool in = j < v;
-        const bool cj = in && ((units[j >> 5] >> (j & 31)) & 1u);
-        const int L = in ? (cj ? nbits : W) : 0;
-        int incl = L;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (in) {
-            const U y = get_bits<U>(stream, base + incl - L, L);
-            U x = y;
-            if (cj) {
-                if (stride == 0)
-                    x = (U)(bv | scatter_regs<U>(y, (U)~m, mv));
-                else
-                    x = (U)(bv | scatter_bits<U>(y, (U)~m, mv, stride));
-            }
-            orow[j] = x;
-        }
-        base += __shfl_sync(0xffffffffu, incl, 31);
-    };
     if constexpr (NC > 0) {
+        int64_t base = 0;
 #pragma unroll
-        for (int c = 0; c < NC; ++c)
-            if (32 * c < v) chunk(32 * c, lt.m[c], lt.bv[c], lt.nb[c], lt.mv[c], 0);
-    } else {
-        for (int64_t c0 = 0; c0 < v; c0 += 32) {
-            const int64_t j = c0 + lane;
+        for (int c = 0; c < NC; ++c) {
+            if (32 * c >= v) break;
+            const int64_t j = 32 * c + lane;
             const bool in = j < v;
-            chunk(c0, in ? __ldg(&t.mask[j]) : (U)0, in ? __ldg(&t.bitval[j]) : (U)0,
-                  in ? (int)__ldg(&t.nb[j]) : 0, t.mv + (in ? j : 0), (int)v);
+            const bool cj = in && ((units[j >> 5] >> (j & 31)) & 1u);
+            const int L = in ? (cj ? lt.nb[c] : W) : 0;
+            int incl = L;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (in) {
+                const U y = get_bits<U>(stream, base + incl - L, L);
+                orow[j] = cj ? (U)(lt.bv[c] | scatter_regs<U>(y, (U)~lt.m[c], lt.mv[c])) : y;
+            }
+            base += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    } else {
+        constexpr int G = 4;
+        int64_t base = 0;
+        for (int64_t g0 = 0; g0 < v; g0 += 32 * G) {
+            U m[G], bv[G];
+            bool in[G], cj[G];
+            int len[G], incl[G];
+#pragma unroll
+            for (int c = 0; c < G; ++c) {
+                const int64_t j = g0 + 32 * c + lane;
+                in[c] = j < v;
+                m[c] = in[c] ? __ldg(&t.mask[j]) : (U)0;
+                bv[c] = in[c] ? __ldg(&t.bitval[j]) : (U)0;
+                const int nb = in[c] ? (int)__ldg(&t.nb[j]) : 0;
+                cj[c] = in[c] && ((units[j >> 5] >> (j & 31)) & 1u);
+                len[c] = in[c] ? (cj[c] ? nb : W) : 0;
+                incl[c] = len[c];
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+                for (int c = 0; c < G; ++c) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl[c], o);
+                    if (lane >= o) incl[c] += y;
+                }
+            }
+            int64_t cb = base;
+#pragma unroll
+            for (int c = 0; c < G; ++c) {
+                const int64_t j = g0 + 32 * c + lane;
+                if (in[c]) {
+                    const U y = get_bits<U>(stream, cb + incl[c] - len[c], len[c]);
+                    orow[j] = cj[c] ? (U)(bv[c] | scatter_bits<U>(y, (U)~m[c], t.mv + j, (int)v))
+                                    : y;
+                }
+                cb += __shfl_sync(0xffffffffu, incl[c], 31);
+            }
+            base = cb;
         }
     }
 }
