@@ -21,8 +21,8 @@
 //    index order (cub radix sort on only the bits the row count needs) so concurrent warps
 //    read neighbouring host pages; fixed-stride compressed rows in HBM, and sparse batches of
 //    them in host memory, where order gains little, claim rows in an open-addressing hash
-//    table instead of sorting.  Repeats are filled
-//    afterwards by a copy kernel (Zipf mini-batches repeat hot rows a lot).
+//    table instead of sorting.  Repeats are filled afterwards by a copy kernel (Zipf
+//    mini-batches repeat hot rows a lot).
 //  * no allocation, no host synchronisation: everything lives in the caller's workspace
 //    and is enqueued on the caller's stream.
 #include <cub/device/device_radix_sort.cuh>
@@ -93,16 +93,20 @@ __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
 }
 
 // Repeats of a hashed fetch: each position whose row another position claimed copies that
-// position's output row (a warp per row copy, 16-byte moves when both rows are aligned).
+// position's output row.  A warp copies the repeats among its 32 positions four rows at a
+// time (all four rows' loads before any store, 16-byte moves when the rows are aligned), so
+// the copies' load latencies overlap.
 template <typename U>
 __global__ void __launch_bounds__(256)
 fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
                    const int64_t *__restrict__ hkeys, const int64_t *__restrict__ hpos,
                    int64_t hslots, U *__restrict__ out, int64_t v) {
+    constexpr int R = 4;
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t bytes = v * (int64_t)sizeof(U);
+    const bool vec_rows = (bytes & 15) == 0 && (((uintptr_t)out) & 15) == 0;
     for (int64_t k0 = warp * 32; k0 < nrows; k0 += nwarps * 32) {
         const int64_t k = k0 + lane;
         const int64_t key = k < nrows ? idx[k] : -1;
@@ -110,16 +114,42 @@ fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
         if (key >= 0 && key < n) hp = hash_find(hkeys, hpos, hslots, key);
         unsigned dm = __ballot_sync(0xffffffffu, hp >= 0 && hp != k);
         while (dm) {
-            const int j = __ffs(dm) - 1;
-            dm &= dm - 1;
-            const U *src = out + __shfl_sync(0xffffffffu, hp, j) * v;
-            U *dst = out + (k0 + j) * v;
-            if (((((uintptr_t)src) | ((uintptr_t)dst)) & 15) == 0 && (bytes & 15) == 0) {
-                const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
-                uint4 *d4 = reinterpret_cast<uint4 *>(dst);
-                for (int64_t q = lane; q < bytes / 16; q += 32) d4[q] = s4[q];
+            const U *src[R];
+            U *dst[R];
+            int cnt = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                src[r] = out;
+                dst[r] = out;
+                if (dm) {
+                    const int j = __ffs(dm) - 1;
+                    dm &= dm - 1;
+                    src[r] = out + __shfl_sync(0xffffffffu, hp, j) * v;
+                    dst[r] = out + (k0 + j) * v;
+                    cnt = r + 1;
+                }
+            }
+            if (vec_rows) {
+                const int64_t n16 = bytes / 16;
+                for (int64_t q = lane; q < n16; q += 32) {
+                    uint4 t[R];
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (r < cnt) t[r] = reinterpret_cast<const uint4 *>(src[r])[q];
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
+                }
             } else {
-                for (int64_t q = lane; q < v; q += 32) dst[q] = src[q];
+                for (int64_t q = lane; q < v; q += 32) {
+                    U t[R];
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (r < cnt) t[r] = src[r][q];
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (r < cnt) dst[r][q] = t[r];
+                }
             }
         }
     }
