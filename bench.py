@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--config", default="graph_features",
                     choices=["graph_features", "embedding_tables", "decoder_layer",
-                             "served_mix", "embedding_bag", "device_rows"])
+                             "served_mix", "embedding_bag", "device_rows", "host_rows"])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=300)
     ap.add_argument("--shard", action="store_true",
@@ -266,6 +266,55 @@ def run_reference_arm(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def setup_vs_reference(torch, ibp, d, x_comp, m, b, bm, sizes):
+    """preprocess (threshold sweep), get_compress_size and compress_inplace of the whole
+    host-resident set, ours against the reference's (built from its sources for sm_100a),
+    each timed on a fresh pinned copy of the uncompressed rows; the reference's masks, sizes,
+    bitmask and compressed bytes are checked against ours bit for bit."""
+    import glob
+    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    y = torch.from_numpy(d).pin_memory()
+
+    def run(pre, size, comp):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mm, bb = pre(y)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        sz = size(y, mm, bb)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        bmk = comp(y, mm, bb)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        ms = {"preprocess_ms": round((t1 - t0) * 1e3, 2),
+              "get_compress_size_ms": round((t2 - t1) * 1e3, 2),
+              "compress_inplace_ms": round((t3 - t2) * 1e3, 2)}
+        return ms, (mm, bb, sz, bmk)
+
+    ours, _ = run(lambda t: ibp.preprocess(t, None), lambda t, mm, bb: ibp.get_compress_size(t, mm, bb),
+                  lambda t, mm, bb: ibp.compress_inplace(t, mm, bb))
+    res = {"ours": ours, "what": "whole 1.2 GB host-resident set, fresh pinned copy each, "
+                                 "wall time with device synchronisation"}
+    if mods:
+        sys.path.insert(0, os.path.dirname(mods[0]))
+        import ibp_cuda as ref
+        ref.print_debug(False)
+        y.copy_(torch.from_numpy(d))
+        theirs, (rm, rb, rsz, rbm) = run(
+            lambda t: ref.preprocess(t, None),
+            lambda t, mm, bb: ref.get_compress_size(t, mm, bb, None, None),
+            lambda t, mm, bb: ref.compress_inplace(t, mm, bb, None))
+        res["reference"] = theirs
+        res["bit_exact_vs_reference"] = bool(
+            torch.equal(rm.cpu(), m.cpu()) and torch.equal(rb.cpu(), b.cpu())
+            and torch.equal(rsz.cpu(), sizes.cpu()) and torch.equal(rbm.cpu(), bm.cpu())
+            and torch.equal(y, x_comp))
+        res["speedup"] = {k: round(theirs[k] / max(ours[k], 1e-6), 2) for k in ours}
+    del y
+    return res
+
+
 def reference_gpu(torch, comp, m, b, bm, comp_len, batches_dev, steps):
     """The reference extension (built from its sources for sm_100a, oracle/_ref) on the same
     compressed rows, through its own positional API; None when it is not built."""
@@ -328,8 +377,9 @@ def run_batched(args):
         x = torch.from_numpy(a).pin_memory()
         m, b = ibp.preprocess(x, thr)
         sizes.append(ibp.get_compress_size(x, m, b))
+        cl = ibp.get_single_compress_len(x, m, b)  # of the uncompressed rows
         bm = ibp.compress_inplace(x, m, b)
-        sets.append((x, m, b, bm, ibp.get_single_compress_len(x, m, b)))
+        sets.append((x, m, b, bm, cl))
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t0
     sizes = [sz.numpy().copy() for sz in sizes]
@@ -550,13 +600,15 @@ def run_embedding_bag(args):
     print(json.dumps(line), flush=True)
 
 
-def run_device_rows(args):
-    """The reference's device-resident decompression benchmark (tests/dev_decomp_thput.py):
-    100,000 int32 rows of 256, 1024 and 4096 bytes (all zeros) compressed in HBM under
-    random masks that make a target share of the bits invariant (12.5% .. 97%), decompressed
-    whole (no index).  Our decompress_fetch against the reference's own (built from its
-    sources for sm_100a, its script's 320 blocks x 512 threads, impls 0 and 1) and a plain
-    clone of the uncompressed rows; CUDA-event times, bit-exact checks on every output."""
+def run_rows(args, where):
+    """The reference's whole-set decompression benchmarks: tests/dev_decomp_thput.py
+    (where="device": rows in HBM, 256/1024/4096-byte rows, against a clone of the raw rows)
+    and tests/decompression_thput.py (where="host": rows in pinned host memory, 256 B-16 KiB
+    rows, against a plain host-to-device copy of the raw rows).  100,000 int32 rows, all
+    zeros, compressed under random masks that make a target share of the bits invariant
+    (12.5% .. 97%), decompressed whole (no index) onto the GPU.  Our decompress_fetch against
+    the reference's own (built from its sources for sm_100a, its scripts' launch settings,
+    impl 0) and the raw copy; CUDA-event times, every output checked bit for bit."""
     import glob
     import torch
     torch.cuda.set_device(0)
@@ -571,8 +623,11 @@ def run_device_rows(args):
         ref.print_debug(False)
     num = 100_000
     rng = np.random.default_rng(11)
-    reps = max(3, min(args.steps, 20))
+    host = where == "host"
+    sizes_b = (256, 1024, 4096, 16384) if host else (256, 1024, 4096)
+    reps = max(3, min(args.steps, 5 if host else 20))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dev = torch.device("cuda")
 
     def timed(fn):
         for _ in range(max(args.warmup, 1)):
@@ -585,69 +640,82 @@ def run_device_rows(args):
         e1.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    def place(t):
+        return t.pin_memory() if host else t.to(dev)
+
     points, launches = [], 0
     with Clocks(torch.cuda.current_device()) as clk:
-        for size in (256, 1024, 4096):
+        for size in sizes_b:
             v = size // 4
-            t = torch.zeros((num, v), dtype=torch.int32, device="cuda")
-            clone_ms = timed(lambda: t.clone())
+            t = place(torch.zeros((num, v), dtype=torch.int32))
+            copy_ms = timed((lambda: t.to(dev, non_blocking=True)) if host else (lambda: t.clone()))
+            want = torch.zeros((num, v), dtype=torch.int32, device=dev)
             for rate in (0.125, 0.25, 0.5, 0.75, 0.9, 0.95, 0.97):
                 # mask bits drawn at random until rate x row bits (+ V + 1) are set; bitval
-                # row 0 (zeros), as the reference script makes them
+                # row 0 (zeros), as the reference scripts make them
                 bits = 32 * v
                 sel = rng.permutation(bits)[:min(bits, int(rate * bits) + v + 1)]
                 mw = np.zeros(v, np.uint32)
                 np.bitwise_or.at(mw, sel // 32, np.uint32(1) << (sel % 32).astype(np.uint32))
-                mask = torch.from_numpy(mw.view(np.int32)).cuda()
-                bitval = torch.zeros(v, dtype=torch.int32, device="cuda")
+                mask = torch.from_numpy(mw.view(np.int32)).to(dev)
+                bitval = torch.zeros(v, dtype=torch.int32, device=dev)
                 x = t.clone()
-                comp_frac = float(ibp.get_compress_size(x, mask, bitval).sum()) / (num * size)
+                x = x.pin_memory() if host else x
+                szs = ibp.get_compress_size(x, mask, bitval)
+                torch.cuda.synchronize()  # host-resident sizes are written asynchronously
+                comp_frac = float(szs.sum()) / (num * size)
+                cl = ibp.get_single_compress_len(x, mask, bitval)  # before compressing
                 bm = ibp.compress_inplace(x, mask, bitval)
-                cl = ibp.get_single_compress_len(x, mask, bitval)
-                out = torch.empty_like(t)
+                out = torch.empty((num, v), dtype=torch.int32, device=dev)
                 l0 = lib.ibp_kernel_launch_count()
-                ours = timed(lambda: ibp.decompress_fetch(x, mask, bitval, bm, "cuda", cl, None,
+                ours = timed(lambda: ibp.decompress_fetch(x, mask, bitval, bm, dev, cl, None,
                                                           output_tensor=out))
                 launches += lib.ibp_kernel_launch_count() - l0
-                assert torch.equal(out, t), "device-rows mismatch"
+                assert torch.equal(out, want), "rows mismatch"
                 pt = {"row_bytes": size, "invariant_target": rate,
                       "compressed_fraction": round(comp_frac, 4),
-                      "ours_us": round(ours * 1e3, 1), "clone_us": round(clone_ms * 1e3, 1),
-                      "ours_GBps": round(num * size / ours / 1e6, 1)}
+                      "ours_us": round(ours * 1e3, 1), "copy_us": round(copy_ms * 1e3, 1),
+                      "ours_GBps": round(num * size / ours / 1e6, 1),
+                      "speedup_vs_copy": round(copy_ms / ours, 2)}
+                del x
                 if ref is not None:
-                    for impl in (0, 1):
-                        xr = t.clone()
-                        bmr = ref.compress_inplace(xr, mask, bitval, None)
-                        holder = {}
+                    xr = t.clone()
+                    xr = xr.pin_memory() if host else xr
+                    bmr = ref.compress_inplace(xr, mask, bitval, None)
+                    holder = {}
+                    nb, nt = (None, None) if host else (320, 512)
 
-                        def rcall():
-                            holder["o"] = ref.decompress_fetch(xr, mask, bitval, bmr,
-                                                               torch.device("cuda"), cl, None,
-                                                               320, 512, impl, None)
-                        rt = timed(rcall)
-                        pt[f"ref_impl{impl}_us"] = round(rt * 1e3, 1)
-                        pt[f"ref_impl{impl}_exact"] = bool(torch.equal(holder["o"], t))
-                    pt["speedup_vs_ref_impl0"] = round(pt["ref_impl0_us"] / pt["ours_us"], 2)
+                    def rcall():
+                        holder["o"] = ref.decompress_fetch(xr, mask, bitval, bmr, dev, cl, None,
+                                                           nb, nt, 0, None)
+                    rt = timed(rcall)
+                    pt["ref_us"] = round(rt * 1e3, 1)
+                    pt["ref_exact"] = bool(torch.equal(holder["o"], want))
+                    pt["speedup_vs_ref"] = round(rt / ours, 2)
+                    del xr, holder
                 points.append(pt)
-                del x, out
-            del t
+                del out
+            del t, want
             torch.cuda.empty_cache()
     head = [p for p in points if p["row_bytes"] == 1024 and p["invariant_target"] == 0.5][0]
-    sp = [p["speedup_vs_ref_impl0"] for p in points if "speedup_vs_ref_impl0" in p]
+    sp = [p["speedup_vs_ref"] for p in points if "speedup_vs_ref" in p]
+    name = ("device-resident decompress delivered GB/s (100k rows in HBM, no index; reference "
+            "dev_decomp_thput pattern)" if not host else
+            "host-resident decompress delivered GB/s (100k pinned rows, no index; reference "
+            "decompression_thput pattern)")
     line = {
-        "metric": "device-resident decompress delivered GB/s (100k rows in HBM, no index; "
-                  "reference dev_decomp_thput pattern)",
-        "value": head["ours_GBps"], "unit": "GB/s", "n_gpus": 1, "steps": reps,
-        "warmup": args.warmup, "ms_per_step": round(head["ours_us"] / 1e3, 4),
+        "metric": name, "value": head["ours_GBps"], "unit": "GB/s", "n_gpus": 1,
+        "steps": reps, "warmup": args.warmup, "ms_per_step": round(head["ours_us"] / 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic",
-        "config": {"workload": "device_rows: 100,000 zero int32 rows of 256/1024/4096 B in HBM, "
-                               "random masks at 7 invariant-bit targets; line value = 1024 B "
-                               "rows at 50%", "l2": "outputs 25-410 MB; 1024/4096 B sets "
-                                                   "exceed L2"},
-        "speedup_vs_ref_impl0": {"min": min(sp) if sp else None,
-                                 "geomean": round(float(np.exp(np.mean(np.log(sp)))), 2)
-                                 if sp else None, "max": max(sp) if sp else None},
+        "config": {"workload": f"{where}_rows: 100,000 zero int32 rows of "
+                               f"{'/'.join(str(z) for z in sizes_b)} B "
+                               f"{'pinned on the host' if host else 'in HBM'}, random masks "
+                               "at 7 invariant-bit targets; line value = 1024 B rows at 50%",
+                   "l2": "sets of 25 MB-1.6 GB; 1024 B rows and up exceed L2"},
+        "speedup_vs_ref": {"min": min(sp) if sp else None,
+                           "geomean": round(float(np.exp(np.mean(np.log(sp)))), 2)
+                           if sp else None, "max": max(sp) if sp else None},
         "points": points,
         "clocks": clk.summary(),
         "gpu_launches": int(launches),
@@ -675,9 +743,10 @@ def served_sets(torch, ibp):
         d = np.ascontiguousarray(f.reshape(-1)[:rows * v * 2]).view(np.int64).reshape(rows, v)
         x = torch.from_numpy(d).pin_memory()
         m, b = ibp.preprocess(x, None)
+        cl = ibp.get_single_compress_len(x, m, b)  # of the uncompressed rows
         bm = ibp.compress_inplace(x, m, b)
         srcs.append(d)
-        sets.append((x, m, b, bm, ibp.get_single_compress_len(x, m, b)))
+        sets.append((x, m, b, bm, cl))
     return srcs, sets
 
 
@@ -826,12 +895,12 @@ def main():
             return
         run_served(args)
         return
-    if args.config == "device_rows":
+    if args.config in ("device_rows", "host_rows"):
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable": "the device-rows "
-                              "configuration times the reference's GPU build in the same line"}))
+            print(json.dumps({"impl": "reference", "unavailable": "the whole-set configurations "
+                              "time the reference's GPU build in the same line"}))
             return
-        run_device_rows(args)
+        run_rows(args, args.config.split("_")[0])
         return
     if args.config == "embedding_bag":
         if args.impl == "reference":
@@ -1059,6 +1128,12 @@ def main():
                         np.array_equal(rout.cpu().numpy(), d[batches[0]]))
             except Exception as exc:  # reported, not fatal
                 ref_gpu = {"error": repr(exc)[:200]}
+        setup = None
+        if not args.no_reference_gpu:
+            try:
+                setup = setup_vs_reference(torch, ibp, d, x, m, b, bm, sizes)
+            except Exception as exc:  # reported, not fatal
+                setup = {"error": repr(exc)[:200]}
         cpu = cpu_baseline(d, m.cpu().numpy(), b.cpu().numpy(), x.numpy(), bm.cpu().numpy(),
                            batches, args.cpu_seconds)
         gather = host_gather_copy_baseline(torch, d, batches)
@@ -1099,6 +1174,7 @@ def main():
                                                 "sort and repeat fill"},
             "condensed": condensed,
             "reference_gpu": ref_gpu,
+            "setup_vs_reference": setup,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }

@@ -51,6 +51,7 @@ struct FetchArgs {
     int64_t slot_words;   // shared-memory words per row slot
     int slots;            // row slots per warp (<= kRowsInFlight)
     int upos;             // positions per chunk the grid was sized for (unit_positions)
+    int gmax;             // largest chunk a warp takes (positions); 0: its row slots
     int64_t *hkeys;       // hashed dedup: open-addressing table of rows (-1 = empty) ...
     int64_t *hpos;        // ... and the position that claimed each (nullptr: no table)
     int64_t hslots;       // the table's slots
@@ -170,7 +171,8 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         // guided self-scheduling: 32-position chunks while much work remains, shrinking to
         // 4 towards the end, so that the grid's last chunks (each a chain of dependent
         // reads) finish close together
-        const int g = (int)min((int64_t)32, max((int64_t)4, (a.nrows - seen) / (2 * nwarps)));
+        const int g = (int)min((int64_t)a.gmax,
+                               max((int64_t)min(4, a.gmax), (a.nrows - seen) / (2 * nwarps)));
         unsigned long long c = 0;
         if (lane == 0) c = atomicAdd(a.work, (unsigned long long)g);
         const int64_t k0 = (int64_t)__shfl_sync(0xffffffffu, c, 0);
@@ -295,6 +297,9 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
         blocks = (int64_t)device_sm_count() * per_sm;
     }
     a.upos = unit_positions(a.nrows, blocks * (threads / 32));
+    // host rows: a warp takes no more positions than it has row slots, so the rows the
+    // whole grid has in flight stay close together in host memory; HBM rows: 32
+    if (a.gmax <= 0) a.gmax = a.slots;
     const int64_t chunks = (a.nrows + a.upos - 1) / a.upos;
     const int64_t need = (chunks + threads / 32 - 1) / (threads / 32);
     if (blocks > need) blocks = need;
@@ -321,7 +326,17 @@ static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStre
         a.slot_words = (int64_t)align_up((size_t)a.s.v + 2 * per16 + 2, per16);
         return launch_fetch_x<U, true>(a, nblks, nthreads, st);
     }
-    a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, per16);
+    if (a.raw_only) {
+        a.slot_words = per16;  // raw rows are copied straight to the output
+    } else if (a.s.v > 256) {
+        // long rows: slots for rows up to twice the first read (the average length when the
+        // caller gives a hint); longer rows decode from their source.  Smaller slots leave
+        // room for more warps per SM and for the column tables in L1.
+        const int64_t cap = std::max<int64_t>(2 * a.s.first_words, 256);
+        a.slot_words = (int64_t)align_up((size_t)std::min<int64_t>(a.s.v, cap) + 2, per16);
+    } else {
+        a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, per16);
+    }
     return launch_fetch_x<U, false>(a, nblks, nthreads, st);
 }
 
@@ -347,7 +362,16 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     if (nrows <= 0 || v <= 0) return IBP_OK;
     if (impl != 2) IBP_RET(build_tables<U>(mask, bitval, v, t, st));
 
+    bool on_device = false;
+    {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, comp) == cudaSuccess)
+            on_device = pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged;
+        else
+            cudaGetLastError();
+    }
     FetchArgs<U> a{};
+    a.gmax = on_device ? 32 : 0;
     a.s.comp = comp;
     a.s.n = n;
     a.s.v = v;
@@ -369,14 +393,6 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         return IBP_ERR_UNSUPPORTED;
     }
     const int mode = fetch_dedup_mode();
-    bool on_device = false;
-    {
-        cudaPointerAttributes pa{};
-        if (cudaPointerGetAttributes(&pa, comp) == cudaSuccess)
-            on_device = pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged;
-        else
-            cudaGetLastError();
-    }
     if (mode == 2 || (mode == 0 && !offsets && impl != 2 && (on_device || 4 * nidx < n))) {
         // fixed-stride compressed rows in HBM, or a sparse batch of them in host memory:
         // claim rows in a hash table instead of sorting (HBM does not care about row order,

@@ -128,6 +128,7 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
             U m[G], bv[G];
             bool in[G], cj[G];
             int len[G], incl[G];
+            bool few = true;  // every column of the group keeps at most 4 bits
 #pragma unroll
             for (int c = 0; c < G; ++c) {
                 const int64_t j = g0 + 32 * c + lane;
@@ -135,10 +136,12 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
                 m[c] = in[c] ? __ldg(&t.mask[j]) : (U)0;
                 bv[c] = in[c] ? __ldg(&t.bitval[j]) : (U)0;
                 const int nb = in[c] ? (int)__ldg(&t.nb[j]) : 0;
+                few = few && nb <= 4;
                 cj[c] = in[c] && ((units[j >> 5] >> (j & 31)) & 1u);
                 len[c] = in[c] ? (cj[c] ? nb : W) : 0;
                 incl[c] = len[c];
             }
+            few = __all_sync(0xffffffffu, few);
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
@@ -148,15 +151,40 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
                 }
             }
             int64_t cb = base;
+            if (few) {
+                // highly invariant columns: place each kept bit from the mask directly
+                // (at most 4 steps, no move-mask loads)
 #pragma unroll
-            for (int c = 0; c < G; ++c) {
-                const int64_t j = g0 + 32 * c + lane;
-                if (in[c]) {
-                    const U y = get_bits<U>(stream, cb + incl[c] - len[c], len[c]);
-                    orow[j] = cj[c] ? (U)(bv[c] | scatter_bits<U>(y, (U)~m[c], t.mv + j, (int)v))
-                                    : y;
+                for (int c = 0; c < G; ++c) {
+                    const int64_t j = g0 + 32 * c + lane;
+                    if (in[c]) {
+                        const U y = get_bits<U>(stream, cb + incl[c] - len[c], len[c]);
+                        U x = y;
+                        if (cj[c]) {
+                            U sel = (U)~m[c], r = 0;
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) {  // nb <= 4: sel is empty after
+                                const U low = (U)(sel & (U)(~sel + 1));
+                                r |= ((y >> i) & 1) ? low : (U)0;
+                                sel &= (U)(sel - 1);
+                            }
+                            x = (U)(bv[c] | r);
+                        }
+                        orow[j] = x;
+                    }
+                    cb += __shfl_sync(0xffffffffu, incl[c], 31);
                 }
-                cb += __shfl_sync(0xffffffffu, incl[c], 31);
+            } else {
+#pragma unroll
+                for (int c = 0; c < G; ++c) {
+                    const int64_t j = g0 + 32 * c + lane;
+                    if (in[c]) {
+                        const U y = get_bits<U>(stream, cb + incl[c] - len[c], len[c]);
+                        orow[j] = cj[c] ? (U)(bv[c] | scatter_bits<U>(y, (U)~m[c], t.mv + j, (int)v))
+                                        : y;
+                    }
+                    cb += __shfl_sync(0xffffffffu, incl[c], 31);
+                }
             }
             base = cb;
         }
@@ -262,7 +290,8 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
                     const U *row = s.comp + r * v;
                     U *buf = slots + q * slot_words;
                     end[q] = row_words<U, NC>(buf, v, s.mw, s.t, lt);
-                    if (end[q] < v && end[q] > s.first_words) {
+                    // a row too long for its slot is decoded straight from its source below
+                    if (end[q] < v && end[q] > s.first_words && end[q] + 2 <= slot_words) {
                         const int64_t b0 = s.first_words / per16;
                         const int64_t b1 = (end[q] + per16 - 1) / per16;
                         if ((((uintptr_t)row) & 15) == 0 && b1 - b0 <= 32) {
@@ -296,6 +325,14 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
                     // a bitmap claiming a stream as long as the raw row cannot come from this
                     // mask: report it and leave the output row alone
                     if (lane == 0) atomicOr(status, kStatusCorruptRow);
+                    continue;
+                }
+                if (end[q] + 2 > slot_words) {
+                    // longer than the slot (slots are sized for rows near the average length
+                    // when rows are long): decode from the source row, whose words after the
+                    // stream are its zero padding
+                    decode_row<U, NC>(s.comp + r * v, v, s.mw, s.t, lt, o);
+                    __syncwarp();
                     continue;
                 }
                 U *buf = slots + q * slot_words;
@@ -506,11 +543,12 @@ fill_repeats_kernel(const int64_t *__restrict__ keys, int64_t nrows, Rows rows) 
     }
 }
 
-// Words of the first read of a compressed row: the caller's average-length hint plus one
-// word, rounded up to whole 32-byte sectors; without a hint, the first 128 bytes.
+// Words of the first read of a compressed row: the caller's average-length hint rounded up
+// to whole 32-byte sectors (a row of exactly the hint's length, e.g. one full 128-byte line,
+// costs one request); without a hint, the first 128 bytes.
 inline int64_t first_read_words(int64_t v, int64_t mw, int wb, int comp_len) {
     const int64_t sector = 32 / wb;
-    int64_t want = (comp_len > 0 && comp_len < v) ? (int64_t)comp_len + 1 : 128 / wb;
+    int64_t want = (comp_len > 0 && comp_len < v) ? (int64_t)comp_len : 128 / wb;
     if (want < mw + 1) want = mw + 1;
     want = (want + sector - 1) / sector * sector;
     return want < v ? want : v;

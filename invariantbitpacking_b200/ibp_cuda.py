@@ -117,7 +117,7 @@ def preprocess_kmeans(dataset, num_clusters, threshold_=None, *, seed_rows=None)
     with torch.cuda.device(dev):
         masks = torch.empty((c, v), dtype=_INT_DTYPE[wb], device=dev)
         bitvals = torch.empty((c, v), dtype=_INT_DTYPE[wb], device=dev)
-        clusters = torch.zeros(n, dtype=torch.int32).pin_memory()
+        clusters = torch.zeros(n, dtype=torch.int32, pin_memory=True)
         need = _lib.ibp_preprocess_kmeans_workspace_size(n, v, wb, c)
         if dataset.device.type != "cuda" and _stage_budget(n * v * wb, dev):
             need += (n * v * wb + 255) // 256 * 256
@@ -180,9 +180,10 @@ def get_compress_size(dataset, mask, bitval, index_array_=None, compress_ctr_=No
         _torch_check(ctr.dim() == 1 and ctr.shape[0] == 1, "Compress ctr should be a single element")
     dev = _cuda_device(dataset, mask, idx)
     with torch.cuda.device(dev):
-        sizes = torch.empty(nrows, dtype=torch.int64, device=dataset.device)
-        if dataset.device.type != "cuda":
-            sizes = sizes.pin_memory()
+        if dataset.device.type != "cuda":  # pinned from the start: no pageable copy
+            sizes = torch.empty(nrows, dtype=torch.int64, pin_memory=True)
+        else:
+            sizes = torch.empty(nrows, dtype=torch.int64, device=dataset.device)
         total = None
         if ctr is not None:
             total = ctr if (ctr.device.type == "cuda" and ctr.dtype == torch.int64) else \
@@ -229,9 +230,10 @@ def compress_condensed(dataset, mask, bitval, index_array_=None):
         _check(_lib.ibp_condensed_offsets(_ptr(offs), nrows, _ptr(total), _ptr(ws), wsb,
                                           _stream()))
         nbytes = int(total.item())  # synchronises, as the reference does
-        comp = torch.zeros(nbytes // wb, dtype=dataset.dtype, device=dataset.device)
         if dataset.device.type != "cuda":
-            comp = comp.pin_memory()
+            comp = torch.zeros(nbytes // wb, dtype=dataset.dtype, pin_memory=True)
+        else:
+            comp = torch.zeros(nbytes // wb, dtype=dataset.dtype, device=dataset.device)
         ws2, wsb2 = _workspace(_lib.ibp_compress_condensed_workspace_size(v, wb), dev)
         _check(_lib.ibp_compress_condensed(_ptr(dataset), n, v, wb, _ptr(mask), _ptr(bitval),
                                            _ptr(idx), -1 if idx is None else nrows, _ptr(offs),
@@ -288,7 +290,8 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
                      "Output tensor shape does not match expected decompressed shape")
         out = output_tensor
     else:
-        out = torch.empty((nrows, v), dtype=comp_dataset.dtype, device=out_device)
+        out = torch.empty((nrows, v), dtype=comp_dataset.dtype, device=out_device,
+                          pin_memory=out_device.type != "cuda")
     if out_device.type != "cuda" and not out.is_pinned():
         out = out.pin_memory()
     dev = _cuda_device(comp_dataset, mask, idx, out)
@@ -356,7 +359,8 @@ def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, out_device
                      "Output tensor shape does not match expected decompressed shape")
         out = output_tensor
     else:
-        out = torch.empty((nrows, v), dtype=comp.dtype, device=out_device)
+        out = torch.empty((nrows, v), dtype=comp.dtype, device=out_device,
+                          pin_memory=out_device.type != "cuda")
     if out_device.type != "cuda" and not out.is_pinned():
         out = out.pin_memory()
     dev = _cuda_device(comp, mask, idx, out)

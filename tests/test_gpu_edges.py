@@ -217,3 +217,37 @@ def test_graph_features_full_size_round_trip(ibp, oracle):
         idx = torch.from_numpy(z.sample(k)).cuda()
         out = ibp.decompress_fetch(x, m, b, bm, "cuda", comp_len, idx)
         assert torch.equal(out, ref[idx])
+
+
+@pytest.mark.parametrize("wb", [4, 8])
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_long_rows_longer_than_their_slot(ibp, oracle, wb, where):
+    """Long rows whose compressed lengths vary a lot around the hint: most rows compress to a
+    few words, a few keep almost every bit, so some rows outgrow the fetch's shared-memory
+    slot (sized from the hint) and are decoded from their source instead; all must match."""
+    rng = np.random.default_rng(21 + wb)
+    n, v = 3000, 1100
+    d = np.zeros((n, v), dtype=np.int64 if wb == 8 else np.int32)
+    noisy = rng.choice(n, 150, replace=False)
+    span = 30 if wb == 8 else 14
+    d[noisy] = rng.integers(0, 1 << span, (noisy.size, v))
+    d[noisy, ::7] = 0  # still compressible: those rows are compressed, but long
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, 0.9)
+    sizes = ibp.get_compress_size(x, m, b)
+    torch.cuda.synchronize()
+    cl = ibp.get_single_compress_len(x, m, b)
+    bm = ibp.compress_inplace(x, m, b)
+    sz = sizes.numpy()
+    assert (sz < v * wb).all() and sz.max() > 4 * cl * wb  # long compressed rows exist
+    if where == "device":
+        x = x.cuda()
+    comp = x.cpu().numpy()
+    idx = np.concatenate([noisy[:40], rng.integers(0, n, 500)])
+    for ix in (None, idx):
+        ti = None if ix is None else torch.from_numpy(ix).cuda()
+        out = ibp.decompress_fetch(x, m, b, bm, "cuda", cl, ti)
+        want = d if ix is None else d[ix]
+        assert np.array_equal(out.cpu().numpy(), want)
+    ref = oracle.decompress(comp, m.cpu().numpy(), b.cpu().numpy(), bm.cpu().numpy(), idx)
+    assert np.array_equal(ref, d[idx])
