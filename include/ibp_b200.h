@@ -306,7 +306,7 @@ ibp_status ibp_server_destroy(ibp_server *srv);
  * ibp_decompress_fetch without nblks/nthreads/impl/workspace; its scratch is a static 4 MiB
  * (4194304-byte) device array that the library reserves on every device that loads it, until
  * the process exits.  A call that needs more scratch than that
- * (ibp_decompress_fetch_workspace_size(...) > 4194304; roughly: more than ~130k index
+ * (ibp_decompress_fetch_workspace_size(...) > 4194304; roughly: more than ~100k index
  * entries) returns IBP_ERR_WORKSPACE before launching anything.  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress, with that device
  * current): make that first call before any stream capture on the device.  All calls share

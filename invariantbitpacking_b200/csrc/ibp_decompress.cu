@@ -52,9 +52,11 @@ struct FetchArgs {
     int slots;            // row slots per warp (<= kRowsInFlight)
     int upos;             // positions per chunk the grid was sized for (unit_positions)
     int gmax;             // largest chunk a warp takes (positions); 0: its row slots
-    int64_t *hkeys;       // hashed dedup: open-addressing table of rows (-1 = empty) ...
-    int64_t *hpos;        // ... and the position that claimed each (nullptr: no table)
+    int64_t *hkeys;       // in-fetch claims: open-addressing table of rows (-1 = empty) ...
+    int64_t *hpos;        // ... and the position that claimed each (nullptr: no claims)
     int64_t hslots;       // the table's slots
+    const int64_t *list;  // positions to fetch (claimed heads), or nullptr: all positions
+    const unsigned long long *list_len;  // entries of `list` (device)
 };
 
 // ------------------------------------------------------------------ hashed dedup
@@ -68,13 +70,19 @@ __device__ __forceinline__ bool hash_claim(int64_t *keys, int64_t *pos, int64_t 
                                            int64_t key, int64_t k) {
     uint64_t h = row_hash(key, slots);
     for (int64_t probe = 0; probe < slots; ++probe) {
-        const unsigned long long old = atomicCAS(
-            reinterpret_cast<unsigned long long *>(keys + h), ~0ull, (unsigned long long)key);
-        if (old == ~0ull) {
-            pos[h] = k;
-            return true;
+        // a plain read first: a row already claimed (hot rows of a skewed batch) costs no
+        // atomic, so repeats do not queue on one address
+        const int64_t cur = *reinterpret_cast<volatile int64_t *>(keys + h);
+        if (cur == key) return false;
+        if (cur == -1) {
+            const unsigned long long old = atomicCAS(
+                reinterpret_cast<unsigned long long *>(keys + h), ~0ull, (unsigned long long)key);
+            if (old == ~0ull) {
+                pos[h] = k;
+                return true;
+            }
+            if ((int64_t)old == key) return false;
         }
-        if ((int64_t)old == key) return false;
         h = h + 1 == (uint64_t)slots ? 0 : h + 1;
     }
     return false;
@@ -91,6 +99,35 @@ __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
         h = h + 1 == (uint64_t)slots ? 0 : h + 1;
     }
     return -1;
+}
+
+// Claim pass of a hashed fetch: every position claims its row; the positions that win are
+// appended to `heads` (one atomic per warp), so the fetch kernel then walks distinct rows
+// only, 32 to a chunk.  Out-of-range rows are flagged here and never claimed.
+__global__ void __launch_bounds__(256)
+claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int64_t *hkeys,
+                   int64_t *hpos, int64_t hslots, int64_t *__restrict__ heads,
+                   unsigned long long *nheads, int32_t *status) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t k0 = warp * 32; k0 < nidx; k0 += nwarps * 32) {
+        const int64_t k = k0 + lane;
+        const int64_t key = k < nidx ? idx[k] : 0;
+        const bool bad = k < nidx && (key < 0 || key >= n);
+        if (bad) atomicOr(status, kStatusBadIndex);
+        const bool ok = k < nidx && !bad;
+        // one claim per distinct row of the warp (the lowest lane holding it)
+        const unsigned same = __match_any_sync(0xffffffffu, ok ? key : (int64_t)-1);
+        const bool first = ok && (__ffs(same) - 1) == lane;
+        const bool head = first && hash_claim(hkeys, hpos, hslots, key, k);
+        const unsigned hm = __ballot_sync(0xffffffffu, head);
+        if (!hm) continue;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(nheads, (unsigned long long)__popc(hm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (head) heads[base + __popc(hm & ((1u << lane) - 1u))] = k;
+    }
 }
 
 // Repeats of a hashed fetch: each position whose row another position claimed copies that
@@ -166,21 +203,23 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
     LaneTables<U, NC> lt;
     if (!a.raw_only) lt.load(a.s.t, a.s.v);
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t nrows = a.list ? (int64_t)*a.list_len : a.nrows;
     int64_t seen = 0;  // positions handed out when this warp last took a chunk
     for (;;) {
         // guided self-scheduling: 32-position chunks while much work remains, shrinking to
         // 4 towards the end, so that the grid's last chunks (each a chain of dependent
         // reads) finish close together
         const int g = (int)min((int64_t)a.gmax,
-                               max((int64_t)min(4, a.gmax), (a.nrows - seen) / (2 * nwarps)));
+                               max((int64_t)min(4, a.gmax), (nrows - seen) / (2 * nwarps)));
         unsigned long long c = 0;
         if (lane == 0) c = atomicAdd(a.work, (unsigned long long)g);
-        const int64_t k0 = (int64_t)__shfl_sync(0xffffffffu, c, 0);
-        if (k0 >= a.nrows) break;
-        seen = k0 + g;
-        // lane-parallel metadata of the chunk's positions
-        const int64_t k = k0 + lane;
-        const bool valid = lane < g && k < a.nrows;
+        const int64_t p0 = (int64_t)__shfl_sync(0xffffffffu, c, 0);
+        if (p0 >= nrows) break;
+        seen = p0 + g;
+        // lane-parallel metadata of the chunk's positions (list entries: claimed heads)
+        const bool valid = lane < g && p0 + lane < nrows;
+        const int64_t k = a.list ? (valid ? a.list[p0 + lane] : 0) : p0 + lane;
+        const int64_t k0 = p0;
         const int64_t key = valid ? (a.keys ? a.keys[k] : k) : -1;
         bool head = valid;
         if (a.dedup) {
@@ -191,7 +230,12 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         const bool bad = head && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         head = head && !bad;
-        if (a.hkeys && head) head = hash_claim(a.hkeys, a.hpos, a.hslots, key, k);
+        if (a.hkeys) {
+            // one claim per distinct row of the chunk (its lowest lane)
+            const unsigned same = __match_any_sync(0xffffffffu, head ? key : (int64_t)-1);
+            head = head && (__ffs(same) - 1) == lane &&
+                   hash_claim(a.hkeys, a.hpos, a.hslots, key, k);
+        }
         U *orow = a.out + (head ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
         if constexpr (EXACT) {
             fetch_heads_exact<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
@@ -264,6 +308,7 @@ size_t decompress_workspace(int64_t nidx, int64_t v, int wb, bool has_index) {
         Sizer hsh;
         hsh.take<int64_t>(hash_slots(nidx));
         hsh.take<int64_t>(hash_slots(nidx));
+        hsh.take<int64_t>(nidx);  // claimed heads
         s.take<char>(std::max(srt.total(), hsh.total()));
     }
     return s.total();
@@ -357,8 +402,9 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     Carver c{(char *)ws, 0, ws_bytes};
     int32_t *status = c.take<int32_t>(kStatusBytes / sizeof(int32_t));
     ColTables<U> t = carve_tables<U>(c, v);
-    // status word (offset 0) and the fetch work counter (offset 64)
-    IBP_CUDA(cudaMemsetAsync(status, 0, 128, st));
+    // status word (offset 0), the fetch work counter (offset 64), the claimed-head count of a
+    // hashed fetch (offset 128)
+    IBP_CUDA(cudaMemsetAsync(status, 0, 192, st));
     if (nrows <= 0 || v <= 0) return IBP_OK;
     if (impl != 2) IBP_RET(build_tables<U>(mask, bitval, v, t, st));
 
@@ -401,11 +447,27 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         const int64_t slots = hash_slots(nidx);
         int64_t *hkeys = c.take<int64_t>(slots);
         int64_t *hpos = c.take<int64_t>(slots);
+        int64_t *heads = c.take<int64_t>(nidx);
         IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, sizeof(int64_t) * slots, st));
         a.keys = idx;
-        a.hkeys = hkeys;
-        a.hpos = hpos;
-        a.hslots = slots;
+        if (on_device) {
+            // HBM rows: claim in a pass of its own, so the fetch walks distinct rows only, 32
+            // to a chunk (the fetch is latency-bound here and chunks of repeats cost it)
+            auto *nheads =
+                reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 128);
+            const int64_t cb =
+                std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
+            claim_heads_kernel<<<(unsigned)cb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
+                                                             heads, nheads, status);
+            IBP_LAUNCHED("claim_heads_kernel");
+            a.list = heads;
+            a.list_len = nheads;
+        } else {
+            // host rows: claims happen inside the fetch, hidden behind its PCIe reads
+            a.hkeys = hkeys;
+            a.hpos = hpos;
+            a.hslots = slots;
+        }
         IBP_RET(launch_fetch<U>(a, nblks, nthreads, st));
         const int64_t fb = std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
         fill_hashed_kernel<U><<<(unsigned)fb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
