@@ -102,17 +102,18 @@ __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
 }
 
 // Claim pass of a hashed fetch: every position claims its row; the positions that win are
-// appended to `heads` (one atomic per warp), so the fetch kernel then walks distinct rows
-// only, 32 to a chunk.  Out-of-range rows are flagged here and never claimed.
+// appended to `heads` (one atomic per block and pass, so the list's counter is not a hot
+// spot), and the fetch kernel then walks distinct rows only, 32 to a chunk.  Out-of-range
+// rows are flagged here and never claimed.  256 threads per block, one position each.
 __global__ void __launch_bounds__(256)
 claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int64_t *hkeys,
                    int64_t *hpos, int64_t hslots, int64_t *__restrict__ heads,
                    unsigned long long *nheads, int32_t *status) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t k0 = warp * 32; k0 < nidx; k0 += nwarps * 32) {
-        const int64_t k = k0 + lane;
+    __shared__ unsigned counts[8];
+    __shared__ unsigned long long block_base;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t b0 = (int64_t)blockIdx.x * 256; b0 < nidx; b0 += (int64_t)gridDim.x * 256) {
+        const int64_t k = b0 + threadIdx.x;
         const int64_t key = k < nidx ? idx[k] : 0;
         const bool bad = k < nidx && (key < 0 || key >= n);
         if (bad) atomicOr(status, kStatusBadIndex);
@@ -122,11 +123,20 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
         const bool first = ok && (__ffs(same) - 1) == lane;
         const bool head = first && hash_claim(hkeys, hpos, hslots, key, k);
         const unsigned hm = __ballot_sync(0xffffffffu, head);
-        if (!hm) continue;
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(nheads, (unsigned long long)__popc(hm));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (head) heads[base + __popc(hm & ((1u << lane) - 1u))] = k;
+        if (lane == 0) counts[wid] = __popc(hm);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned run = 0;
+            for (int w = 0; w < 8; ++w) {
+                const unsigned c = counts[w];
+                counts[w] = run;
+                run += c;
+            }
+            block_base = run ? atomicAdd(nheads, (unsigned long long)run) : 0ull;
+        }
+        __syncthreads();
+        if (head) heads[block_base + counts[wid] + __popc(hm & ((1u << lane) - 1u))] = k;
+        __syncthreads();  // counts and block_base are rewritten by the next pass
     }
 }
 
