@@ -3,26 +3,31 @@
 //
 // B200 design
 //  * rows come from pinned host memory (zero-copy over PCIe) or HBM.  A warp takes a chunk
-//    of 32 consecutive (sorted) positions from a global work counter, loads their keys,
-//    output positions and bitmask bits lane-parallel (one round trip for 32 rows), and then
-//    loads the first read of up to kRowsInFlight distinct rows into registers (16-byte loads,
-//    all rows before any store) and parks them in shared-memory slots, so several PCIe
-//    round trips overlap per warp.
-//  * the first read of a compressed row is sized by the caller's average-length hint
-//    (comp_len), rounded to whole 32-byte sectors: one request per row when the hint holds;
-//    the bitmap then gives the exact length and a second read fetches any remainder.
+//    of consecutive positions from a global work counter (up to its row slots for host
+//    rows, so the rows the grid has in flight stay close together; 32 for HBM rows; fewer
+//    towards the end of the work so the last chunks finish together), loads their keys,
+//    output positions and bitmask bits lane-parallel, and then loads the first read of up
+//    to kRowsInFlight distinct rows into registers (16-byte loads, all rows before any
+//    store) and parks them in shared-memory slots, so several PCIe round trips overlap per
+//    warp; the rows that need more than their first read get their tails the same way.
+//  * the first read of a compressed row is the caller's average-length hint (comp_len)
+//    rounded up to whole 32-byte sectors: one round trip per row when the hint holds.
+//    Rows longer than 256 words get slots for twice the hint only; a row that outgrows its
+//    slot decodes straight from its source.
 //  * decode: lane j of a 32-word chunk takes its bit length, a warp prefix sum gives its
 //    stream offset, a funnel read pulls its bits and the Hacker's Delight scatter places
 //    them at the non-invariant positions (log2(W) branch-free steps).  For rows of up to 64
 //    words the per-column tables (mask, bitval, kept bits, move masks) live in registers,
-//    loaded once per warp; longer rows read them through the L1 cache.
-//  * index arrays: each distinct row crosses PCIe once.  Dense batches of host rows (a
+//    loaded once per warp; longer rows read them through the L1 cache, four chunks at a
+//    time, and place the bits of columns that keep at most 4 directly from the mask.
+//  * index arrays: each distinct row crosses the link once.  Dense batches of host rows (a
 //    quarter of the rows or more), condensed rows and raw gathers are fetched in sorted
 //    index order (cub radix sort on only the bits the row count needs) so concurrent warps
-//    read neighbouring host pages; fixed-stride compressed rows in HBM, and sparse batches of
-//    them in host memory, where order gains little, claim rows in an open-addressing hash
-//    table instead of sorting.  Repeats are filled afterwards by a copy kernel (Zipf
-//    mini-batches repeat hot rows a lot).
+//    read neighbouring host pages.  Fixed-stride compressed rows in HBM, and sparse batches
+//    of them in host memory, where order gains little, claim rows in an open-addressing
+//    hash table instead: inside the fetch for host rows (hidden behind PCIe), in a claim
+//    pass that lists the distinct rows for HBM rows.  Repeats are filled afterwards by a
+//    copy kernel (Zipf mini-batches repeat hot rows a lot).
 //  * no allocation, no host synchronisation: everything lives in the caller's workspace
 //    and is enqueued on the caller's stream.
 #include <cub/device/device_radix_sort.cuh>
