@@ -228,7 +228,7 @@ def host_gather_copy_baseline(torch, d, batches, seconds=5.0):
 
 WORKLOAD = ("graph_features: 2.4M x 128 fp32 N(0,0.3^2), 8 mantissa bits, 30% zeros -> "
             "int64 [2.4M x 64], pinned host (1.2 GB)")
-BATCHES = "Zipf(1.1) mini-batches cycling 100k/200k/400k rows"
+BATCH_DESC = "Zipf(1.1) mini-batches cycling 100k/200k/400k rows"
 
 
 def run_reference_arm(args, ws, rank):
@@ -257,7 +257,7 @@ def run_reference_arm(args, ws, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(el * 1e3 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "vec_words": V, "batches": BATCHES,
+        "config": {"workload": WORKLOAD, "vec_words": V, "batches": BATCH_DESC,
                    "rows": args.rows, "sample_rows_per_step": per_step,
                    "mask": "preprocess sweep on the first 200k rows"},
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s",
@@ -1169,7 +1169,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD,
                        "rows": args.rows, "vec_words": V,
-                       "batches": BATCHES,
+                       "batches": BATCH_DESC,
                        "avg_rows_per_step": nrows_avg, "comp_len_words": comp_len,
                        "compressed_fraction": round(float(sizes_np.sum()) / d.nbytes, 4),
                        "l2": "inputs larger than L2 (1.2 GB host set; 51-205 MB outputs)",
