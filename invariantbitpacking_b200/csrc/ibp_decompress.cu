@@ -57,6 +57,7 @@ struct FetchArgs {
     int slots;            // row slots per warp (<= kRowsInFlight)
     int upos;             // positions per chunk the grid was sized for (unit_positions)
     int gmax;             // largest chunk a warp takes (positions); 0: its row slots
+    bool async_rows;      // rows in device memory: first reads as asynchronous copies
     int64_t *hkeys;       // in-fetch claims: open-addressing table of rows (-1 = empty) ...
     int64_t *hpos;        // ... and the position that claimed each (nullptr: no claims)
     int64_t hslots;       // the table's slots
@@ -210,11 +211,14 @@ fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
 
 // ------------------------------------------------------------------ fetch kernel
 // EXACT: condensed rows (byte ranges from a.s.offsets) instead of fixed-stride rows.
-template <typename U, int NC, bool EXACT>
+// ASYNC: fixed-stride rows in device memory, first reads double-buffered (fetch_heads_async;
+// each warp owns two sets of a.slots slots).
+template <typename U, int NC, bool EXACT, bool ASYNC>
 __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
-    U *slots = reinterpret_cast<U *>(smem) + (int64_t)(threadIdx.x >> 5) * a.slots * a.slot_words;
+    U *slots = reinterpret_cast<U *>(smem) +
+               (int64_t)(threadIdx.x >> 5) * a.slots * (ASYNC ? 2 : 1) * a.slot_words;
     LaneTables<U, NC> lt;
     if (!a.raw_only) lt.load(a.s.t, a.s.v);
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -258,8 +262,12 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         } else {
             const bool packed =
                 head && !a.raw_only && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1);
-            fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head, packed,
-                               a.status);
+            if constexpr (ASYNC)
+                fetch_heads_async<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
+                                         packed, a.status);
+            else
+                fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
+                                   packed, a.status);
         }
     }
 }
@@ -329,9 +337,10 @@ size_t decompress_workspace(int64_t nidx, int64_t v, int wb, bool has_index) {
     return s.total();
 }
 
-template <typename U, int NC, bool EXACT>
+template <typename U, int NC, bool EXACT, bool ASYNC>
 static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaStream_t st) {
-    const size_t slot_bytes = (size_t)a.slot_words * sizeof(U);
+    // a warp's slots: one set, or two for the double-buffered reads of device rows
+    const size_t slot_bytes = (size_t)a.slot_words * sizeof(U) * (ASYNC ? 2 : 1);
     int threads = nthreads > 0 ? nthreads : kFetchThreads;
     threads = threads < 32 ? 32 : (threads > kFetchThreads ? kFetchThreads : threads / 32 * 32);
     const int maxs = device_max_smem_optin();
@@ -347,7 +356,7 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
         return IBP_ERR_UNSUPPORTED;
     }
     a.slots = slots;
-    auto kern = fetch_rows_kernel<U, NC, EXACT>;
+    auto kern = fetch_rows_kernel<U, NC, EXACT, ASYNC>;
     IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int64_t blocks = nblks;
     if (blocks <= 0) {
@@ -370,11 +379,12 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     return IBP_OK;
 }
 
-template <typename U, bool EXACT>
+template <typename U, bool EXACT, bool ASYNC>
 static ibp_status launch_fetch_x(FetchArgs<U> a, int nblks, int nthreads, cudaStream_t st) {
-    if (a.raw_only || a.s.v > 64) return launch_fetch_nc<U, 0, EXACT>(a, nblks, nthreads, st);
-    if (a.s.v > 32) return launch_fetch_nc<U, 2, EXACT>(a, nblks, nthreads, st);
-    return launch_fetch_nc<U, 1, EXACT>(a, nblks, nthreads, st);
+    if (a.raw_only || a.s.v > 64)
+        return launch_fetch_nc<U, 0, EXACT, ASYNC>(a, nblks, nthreads, st);
+    if (a.s.v > 32) return launch_fetch_nc<U, 2, EXACT, ASYNC>(a, nblks, nthreads, st);
+    return launch_fetch_nc<U, 1, EXACT, ASYNC>(a, nblks, nthreads, st);
 }
 
 template <typename U>
@@ -384,7 +394,7 @@ static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStre
     if (a.s.offsets) {
         // a condensed row starts at any word: room for the blocks around it and the padding
         a.slot_words = (int64_t)align_up((size_t)a.s.v + 2 * per16 + 2, per16);
-        return launch_fetch_x<U, true>(a, nblks, nthreads, st);
+        return launch_fetch_x<U, true, false>(a, nblks, nthreads, st);
     }
     if (a.raw_only) {
         a.slot_words = per16;  // raw rows are copied straight to the output
@@ -397,7 +407,8 @@ static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStre
     } else {
         a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, per16);
     }
-    return launch_fetch_x<U, false>(a, nblks, nthreads, st);
+    if (a.async_rows && !a.raw_only) return launch_fetch_x<U, false, true>(a, nblks, nthreads, st);
+    return launch_fetch_x<U, false, false>(a, nblks, nthreads, st);
 }
 
 template <typename U>
@@ -433,6 +444,9 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     }
     FetchArgs<U> a{};
     a.gmax = on_device ? 32 : 0;
+    // HBM rows of 512 bytes and up: first reads double-buffered (smaller rows decode too
+    // quickly for the extra bookkeeping to pay)
+    a.async_rows = on_device && v * (int64_t)sizeof(U) >= 512;
     a.s.comp = comp;
     a.s.n = n;
     a.s.v = v;

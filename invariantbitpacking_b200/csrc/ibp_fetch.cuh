@@ -215,6 +215,88 @@ __device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t 
 }
 
 
+// Second half of a group of rows whose first reads are in their slots (slot q at
+// slots + q * slot_words for the rows of lanes lid[0..cnt)): exact lengths from the
+// bitmaps, the rest of every row that needs more than its first read (all issued before any
+// is waited for: 16-byte blocks in registers, at most 32 per row; longer tails and
+// unaligned rows take the plain loop), then the decode (or copy, for rows stored raw).
+template <typename U, int NC>
+__device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables<U, NC> &lt,
+                                            U *__restrict__ slots, int64_t slot_words,
+                                            const int *lid, int cnt, int64_t key, U *orow,
+                                            bool packed, int32_t *status) {
+    const int lane = threadIdx.x & 31;
+    const int64_t v = s.v;
+    int64_t end[kRowsInFlight];
+    {
+        constexpr int per16 = 16 / sizeof(U);
+        uint4 tail[kRowsInFlight];
+        int64_t tb0[kRowsInFlight], tb1[kRowsInFlight];
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            end[q] = -1;
+            tb0[q] = tb1[q] = 0;
+            if (q < cnt && __shfl_sync(0xffffffffu, (int)packed, lid[q])) {
+                const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+                const U *row = s.comp + r * v;
+                U *buf = slots + q * slot_words;
+                end[q] = row_words<U, NC>(buf, v, s.mw, s.t, lt);
+                // a row too long for its slot is decoded straight from its source below
+                if (end[q] < v && end[q] > s.first_words && end[q] + 2 <= slot_words) {
+                    const int64_t b0 = s.first_words / per16;
+                    const int64_t b1 = (end[q] + per16 - 1) / per16;
+                    if ((((uintptr_t)row) & 15) == 0 && b1 - b0 <= 32) {
+                        tb0[q] = b0;
+                        tb1[q] = b1;
+                        if (b0 + lane < b1)
+                            tail[q] = reinterpret_cast<const uint4 *>(row)[b0 + lane];
+                    } else {
+                        issue_words<U>(buf, row, s.first_words, end[q]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q)
+            if (tb0[q] + lane < tb1[q])
+                reinterpret_cast<uint4 *>(slots + q * slot_words)[tb0[q] + lane] = tail[q];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < kRowsInFlight; ++q) {
+        if (q < cnt) {
+            const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+            U *o = reinterpret_cast<U *>(
+                __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
+            if (end[q] < 0) {
+                warp_copy<U>(o, s.comp + r * v, v);
+                continue;
+            }
+            if (end[q] >= v) {
+                // a bitmap claiming a stream as long as the raw row cannot come from this
+                // mask: report it and leave the output row alone
+                if (lane == 0) atomicOr(status, kStatusCorruptRow);
+                continue;
+            }
+            if (end[q] + 2 > slot_words) {
+                // longer than the slot (slots are sized for rows near the average length
+                // when rows are long): decode from the source row, whose words after the
+                // stream are its zero padding
+                decode_row<U, NC>(s.comp + r * v, v, s.mw, s.t, lt, o);
+                __syncwarp();
+                continue;
+            }
+            U *buf = slots + q * slot_words;
+            // words past the stream read as zero (get_bits looks one word ahead; the
+            // value there never reaches an output bit)
+            if (lane < 2) buf[end[q] + lane] = 0;
+            __syncwarp();
+            decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
+            __syncwarp();
+        }
+    }
+}
+
 // Fetch and decode (or copy, when not packed) the rows of the lanes whose `head` is set:
 // groups of up to `nslots` rows have their first reads, and then the rest of the rows that
 // need it, loaded into registers together (16-byte loads, all rows before any store), so
@@ -273,77 +355,88 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
             }
         }
         __syncwarp();
-        // exact lengths from the bitmaps, then the rest of every row that needs more than its
-        // first read, all issued before any is waited for (16-byte blocks in registers, at
-        // most 32 per row; longer tails and unaligned rows take the plain loop)
-        int64_t end[kRowsInFlight];
-        {
-            constexpr int per16 = 16 / sizeof(U);
-            uint4 tail[kRowsInFlight];
-            int64_t tb0[kRowsInFlight], tb1[kRowsInFlight];
+        finish_rows<U, NC>(s, lt, slots, slot_words, lid, cnt, key, orow, packed, status);
+    }
+}
+
+// The next up-to-`nslots` head lanes of `hm` (removed from it), in lane order.
+__device__ __forceinline__ int pick_rows(unsigned &hm, int nslots, int *lid) {
+    int cnt = 0;
 #pragma unroll
-            for (int q = 0; q < kRowsInFlight; ++q) {
-                end[q] = -1;
-                tb0[q] = tb1[q] = 0;
-                if (q < cnt && __shfl_sync(0xffffffffu, (int)packed, lid[q])) {
-                    const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
-                    const U *row = s.comp + r * v;
-                    U *buf = slots + q * slot_words;
-                    end[q] = row_words<U, NC>(buf, v, s.mw, s.t, lt);
-                    // a row too long for its slot is decoded straight from its source below
-                    if (end[q] < v && end[q] > s.first_words && end[q] + 2 <= slot_words) {
-                        const int64_t b0 = s.first_words / per16;
-                        const int64_t b1 = (end[q] + per16 - 1) / per16;
-                        if ((((uintptr_t)row) & 15) == 0 && b1 - b0 <= 32) {
-                            tb0[q] = b0;
-                            tb1[q] = b1;
-                            if (b0 + lane < b1)
-                                tail[q] = reinterpret_cast<const uint4 *>(row)[b0 + lane];
-                        } else {
-                            issue_words<U>(buf, row, s.first_words, end[q]);
-                        }
-                    }
-                }
+    for (int q = 0; q < kRowsInFlight; ++q) {
+        lid[q] = 0;
+        if (q < nslots && hm) {
+            lid[q] = __ffs(hm) - 1;
+            hm &= hm - 1;
+            ++cnt;
+        }
+    }
+    return cnt;
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// fetch_heads for rows in device memory: the first reads of the next group of rows are
+// issued as asynchronous copies into a second set of slots while the current group is
+// decoded, so a warp's HBM round trips overlap its decode instead of following it (the
+// warp owns 2 x nslots slots).  Not used for host rows: asynchronous copies from host
+// memory are slow on this part.
+template <typename U, int NC>
+__device__ __forceinline__ void fetch_heads_async(const RowSet<U> &s, const LaneTables<U, NC> &lt,
+                                                  U *__restrict__ slots, int nslots,
+                                                  int64_t slot_words, int64_t key, U *orow,
+                                                  bool head, bool packed, int32_t *status) {
+    constexpr int per16 = 16 / sizeof(U);
+    const int lane = threadIdx.x & 31;
+    const int64_t v = s.v;
+    const int64_t nq = (s.first_words + per16 - 1) / per16;
+    auto issue = [&](const int *lid, int cnt, U *base) {
+        for (int q = 0; q < cnt; ++q) {
+            const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+            const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[q]);
+            if (!pk) continue;
+            const U *row = s.comp + r * v;
+            U *buf = base + q * slot_words;
+            if ((((uintptr_t)row) & 15) == 0) {
+                for (int64_t b = lane; b < nq; b += 32)
+                    cp_async16(reinterpret_cast<uint4 *>(buf) + b,
+                               reinterpret_cast<const uint4 *>(row) + b);
+            } else {
+                issue_words<U>(buf, row, 0, s.first_words);
             }
-#pragma unroll
-            for (int q = 0; q < kRowsInFlight; ++q)
-                if (tb0[q] + lane < tb1[q])
-                    reinterpret_cast<uint4 *>(slots + q * slot_words)[tb0[q] + lane] = tail[q];
+        }
+        cp_async_commit();
+    };
+    unsigned hm = __ballot_sync(0xffffffffu, head);
+    int lid[kRowsInFlight], nlid[kRowsInFlight];
+    int cnt = pick_rows(hm, nslots, lid);
+    int cur = 0;
+    if (cnt) issue(lid, cnt, slots);
+    while (cnt) {
+        const int ncnt = pick_rows(hm, nslots, nlid);
+        U *nbase = slots + (int64_t)(cur ^ 1) * nslots * slot_words;
+        if (ncnt) {
+            issue(nlid, ncnt, nbase);
+            cp_async_wait_one();  // the current group's copies are done
+        } else {
+            cp_async_wait_all();
         }
         __syncwarp();
+        finish_rows<U, NC>(s, lt, slots + (int64_t)cur * nslots * slot_words, slot_words, lid,
+                           cnt, key, orow, packed, status);
+        __syncwarp();
 #pragma unroll
-        for (int q = 0; q < kRowsInFlight; ++q) {
-            if (q < cnt) {
-                const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
-                U *o = reinterpret_cast<U *>(
-                    __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
-                if (end[q] < 0) {
-                    warp_copy<U>(o, s.comp + r * v, v);
-                    continue;
-                }
-                if (end[q] >= v) {
-                    // a bitmap claiming a stream as long as the raw row cannot come from this
-                    // mask: report it and leave the output row alone
-                    if (lane == 0) atomicOr(status, kStatusCorruptRow);
-                    continue;
-                }
-                if (end[q] + 2 > slot_words) {
-                    // longer than the slot (slots are sized for rows near the average length
-                    // when rows are long): decode from the source row, whose words after the
-                    // stream are its zero padding
-                    decode_row<U, NC>(s.comp + r * v, v, s.mw, s.t, lt, o);
-                    __syncwarp();
-                    continue;
-                }
-                U *buf = slots + q * slot_words;
-                // words past the stream read as zero (get_bits looks one word ahead; the
-                // value there never reaches an output bit)
-                if (lane < 2) buf[end[q] + lane] = 0;
-                __syncwarp();
-                decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
-                __syncwarp();
-            }
-        }
+        for (int q = 0; q < kRowsInFlight; ++q) lid[q] = nlid[q];
+        cnt = ncnt;
+        cur ^= 1;
     }
 }
 
