@@ -353,6 +353,35 @@ def reference_gpu(torch, comp, m, b, bm, comp_len, batches_dev, steps):
                     "nblks=2*SMs) on the same compressed rows and index arrays"}, out
 
 
+def kmeans_vs_reference(torch, ibp, arrays):
+    """preprocess_kmeans (16 clusters) on the three smallest tables viewed as int32 rows of 64
+    words, ours against the reference's (built from its sources for sm_100a; its 8-byte
+    k-means indexes past a shared array, so it runs on the 4-byte view only).  The same
+    initial centroid rows are used by both (the reference's std::random_shuffle with the
+    process's rand() state, restated by ours); the reference's assignment races on ties, so
+    the masks are not compared here (the tests pin them on tie-free data)."""
+    import glob
+    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    if not mods:
+        return None
+    sys.path.insert(0, os.path.dirname(mods[0]))
+    import ibp_cuda as ref
+    ref.print_debug(False)
+    small = sorted(arrays, key=lambda a: a.shape[0])[:3]
+    views = [torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory() for a in small]
+    res = {"rows": [int(a.shape[0]) for a in small], "words": 64}
+    for name, fn in (("ours_s", lambda t: ibp.preprocess_kmeans(t, 16, None)),
+                     ("reference_s", lambda t: ref.preprocess_kmeans(t, 16, None))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for t in views:
+            fn(t)
+        torch.cuda.synchronize()
+        res[name] = round(time.perf_counter() - t0, 3)
+    res["speedup"] = round(res["reference_s"] / max(res["ours_s"], 1e-9), 2)
+    return res
+
+
 def run_batched(args):
     """One batched, graph-replayed launch per step over many tensor sets, against one
     decompress_fetch call per set (the reference's calling pattern).
@@ -388,12 +417,13 @@ def run_batched(args):
     torch.cuda.synchronize()
     prep_s = time.perf_counter() - t0
     sizes = [sz.numpy().copy() for sz in sizes]
-    km = None
+    km = km_vs_ref = None
     if args.config == "embedding_tables":
         t0 = time.perf_counter()
         for a in arrays:
             ibp.preprocess_kmeans(torch.from_numpy(a).pin_memory(), 16, 0.9)
         km = round(time.perf_counter() - t0, 3)
+        km_vs_ref = kmeans_vs_reference(torch, ibp, arrays)
     nsets = len(sets)
     v = [s[0].shape[1] for s in sets]
     variants = []
@@ -507,7 +537,8 @@ def run_batched(args):
                                                 sum(a.nbytes for a in arrays), 4),
                    "launch_shape": shape, "graph": True,
                    "setup_s": {"generate": round(gen_s, 2), "preprocess_compress": round(prep_s, 2),
-                               "preprocess_kmeans_all_tables": km}},
+                               "preprocess_kmeans_all_tables": km},
+                   "preprocess_kmeans_vs_reference": km_vs_ref},
         "per_call": {"value": round(ptot / pms / 1e6, 3), "unit": "GB/s",
                      "ms_per_step": round(pms / args.steps, 4),
                      "what": f"{nsets} ibp.decompress_fetch calls per step, one per set"},
