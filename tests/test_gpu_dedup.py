@@ -31,7 +31,7 @@ def make(rng, n, v, wb):
     return np.ascontiguousarray(f).view(np.int64 if wb == 8 else np.int32)
 
 
-@pytest.mark.parametrize("wb,v", [(8, 64), (8, 7), (4, 33), (4, 128), (8, 300)])
+@pytest.mark.parametrize("wb,v", [(8, 64), (8, 7), (4, 33), (4, 128), (8, 300), (8, 65), (4, 131)])
 @pytest.mark.parametrize("where", ["host", "device"])
 def test_dedup_modes_match_oracle(ibp, oracle, mode, wb, v, where):
     rng = np.random.default_rng(v * 10 + wb)

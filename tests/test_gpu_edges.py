@@ -251,3 +251,26 @@ def test_long_rows_longer_than_their_slot(ibp, oracle, wb, where):
         assert np.array_equal(out.cpu().numpy(), want)
     ref = oracle.decompress(comp, m.cpu().numpy(), b.cpu().numpy(), bm.cpu().numpy(), idx)
     assert np.array_equal(ref, d[idx])
+
+
+@pytest.mark.parametrize("wb,v", [(8, 64), (8, 65), (4, 131), (8, 600)])
+def test_device_rows_whole_set_and_small_batches(ibp, oracle, wb, v):
+    """Device-resident rows of 512 bytes and up take the double-buffered read path; rows whose
+    length is not a multiple of 16 bytes alternate alignment (the unaligned ones fall back to
+    plain loads).  Whole sets, tiny batches and repeats must all match the oracle."""
+    rng = np.random.default_rng(v + wb)
+    n = 4000
+    f = rng.normal(0, 0.4, (n, v * wb // 4)).astype(np.float32)
+    f = (f.view(np.uint32) & np.uint32(0xFFFF8000)).view(np.float32)
+    d = np.ascontiguousarray(f).view(np.int64 if wb == 8 else np.int32)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    cl = ibp.get_single_compress_len(x, m, b)
+    bm = ibp.compress_inplace(x, m, b)
+    xd = x.cuda()
+    out = ibp.decompress_fetch(xd, m, b, bm, "cuda", cl, None)
+    assert np.array_equal(out.cpu().numpy(), d)
+    for k in (1, 5, 33, 1000):
+        idx = rng.integers(0, n, k)
+        out = ibp.decompress_fetch(xd, m, b, bm, "cuda", cl, torch.from_numpy(idx).cuda())
+        assert np.array_equal(out.cpu().numpy(), d[idx])
