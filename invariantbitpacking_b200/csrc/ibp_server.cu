@@ -302,6 +302,22 @@ static void scheduler(Server *s) {
     }
 }
 
+// Frees every buffer, stream and event a server holds (null ones are skipped) and the server.
+// Its threads must have stopped (or never started).
+static void release_server(Server *s) {
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (char *h : s->tbl_host) cudaFreeHost(h);
+    for (char *d : s->tbl_dev) cudaFree(d);
+    for (cudaEvent_t ev : s->tbl_event) cudaEventDestroy(ev);
+    if (s->idx_host) cudaFreeHost(s->idx_host);
+    if (s->idx_dev) cudaFree(s->idx_dev);
+    if (s->ws) cudaFree(s->ws);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    for (Batch *b : s->inflight) delete b;
+    delete s;
+}
+
 }  // namespace ibp200
 
 using namespace ibp200;
@@ -334,6 +350,7 @@ ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int
     cudaGetDevice(&s->device);
     auto fail = [&](cudaError_t e, const char *what) {
         set_error("server_create: %s: %s", what, cudaGetErrorString(e));
+        release_server(s);  // nothing of a failed creation is kept
         return IBP_ERR_CUDA;
     };
     cudaError_t e;
@@ -344,8 +361,8 @@ ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int
     for (int i = 0; i < max_inflight; ++i) {
         char *h = nullptr, *d = nullptr;
         if ((e = cudaHostAlloc(&h, tbytes, cudaHostAllocDefault)) != cudaSuccess) return fail(e, "table");
-        if ((e = cudaMalloc(&d, tbytes)) != cudaSuccess) return fail(e, "table");
         s->tbl_host.push_back(h);
+        if ((e = cudaMalloc(&d, tbytes)) != cudaSuccess) return fail(e, "table");
         s->tbl_dev.push_back(d);
         s->tbl_busy.push_back(false);
         cudaEvent_t ev = nullptr;
@@ -499,19 +516,7 @@ ibp_status ibp_server_destroy(ibp_server *srv) {
     if (s->thr.joinable()) s->thr.join();
     s->rec_cv.notify_all();
     if (s->done_thr.joinable()) s->done_thr.join();
-    cudaSetDevice(s->device);
-    cudaStreamSynchronize(s->stream);
-    for (size_t i = 0; i < s->tbl_host.size(); ++i) {
-        cudaFreeHost(s->tbl_host[i]);
-        cudaFree(s->tbl_dev[i]);
-    }
-    for (cudaEvent_t ev : s->tbl_event) cudaEventDestroy(ev);
-    cudaFreeHost(s->idx_host);
-    cudaFree(s->idx_dev);
-    cudaFree(s->ws);
-    cudaStreamDestroy(s->stream);
-    for (Batch *b : s->inflight) delete b;
-    delete s;
+    release_server(s);
     return IBP_OK;
 }
 
