@@ -14,7 +14,8 @@ reference row is at least 128 bytes (its warp row copy reads and writes up to
 32 four-byte words past a shorter row) and k-means runs only on 4-byte words
 (its create_mask_many indexes past its shared array for 8-byte words).
 
-Usage (GPU box): python tests/golden/make_golden.py --out gpurun_out/golden
+Usage (on a machine with a B200 and the reference built into oracle/_ref):
+    python tests/golden/make_golden.py --out <dir>   # then copy the .npz files here
 """
 import argparse
 import ctypes
@@ -144,7 +145,7 @@ def random_mask(rng, v, wb, frac):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(REPO, "gpurun_out", "golden"))
+    ap.add_argument("--out", default=os.path.join(REPO, "golden_out"))
     ap.add_argument("--part", choices=["codec", "kmeans"], default="codec")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
