@@ -286,16 +286,20 @@ ibp_status ibp_server_submit(ibp_server *srv, int32_t set, const int64_t *rows, 
  * times[0..2] = submitted, admitted, done.  IBP_ERR_UNSUPPORTED on timeout. */
 ibp_status ibp_server_wait(ibp_server *srv, int64_t id, int32_t timeout_ms, void **out,
                            double *times);
+/* Withdraw a request still queued (not yet admitted): it is not fetched, and waiting for it
+ * afterwards reports an unknown request.  IBP_ERR_UNSUPPORTED once it is admitted. */
+ibp_status ibp_server_cancel(ibp_server *srv, int64_t id);
 /* Give a finished request's output rows back to the arena. */
 ibp_status ibp_server_release(ibp_server *srv, int64_t id);
-/* stats[0..3] = batches launched, rows done, output bytes done, requests pending. */
 /* Admission limits of one batch: at most max_rows rows (no more than the sort workspace's
  * max(index_capacity, 2^20)) and max_bytes output bytes, both counted after the batch's
  * first request, which is always admitted.  <= 0 keeps the current value.  Defaults: the
  * sort workspace's rows and 128 MiB.  Smaller batches finish early requests of a burst
  * sooner (lower p50); larger ones amortise per-launch cost. */
 ibp_status ibp_server_set_batch_limits(ibp_server *srv, int64_t max_rows, int64_t max_bytes);
+/* stats[0..3] = batches launched, rows done, output bytes done, requests pending. */
 ibp_status ibp_server_stats(ibp_server *srv, int64_t *stats);
+/* Stop the scheduler after the in-flight batches finish and free the server's buffers. */
 ibp_status ibp_server_destroy(ibp_server *srv);
 
 /* ---------------------------------------------------------------- decompress_fetch, no allocation

@@ -60,6 +60,7 @@ SIGNATURES = {
     "ibp_server_submit": (_INT, [_P, _I32, _P, _I64, _I64, _P]),
     "ibp_server_wait": (_INT, [_P, _I64, _I32, _P, _P]),
     "ibp_server_release": (_INT, [_P, _I64]),
+    "ibp_server_cancel": (_INT, [_P, _I64]),
     "ibp_server_set_batch_limits": (_INT, [_P, _I64, _I64]),
     "ibp_server_stats": (_INT, [_P, _P]),
     "ibp_server_destroy": (_INT, [_P]),

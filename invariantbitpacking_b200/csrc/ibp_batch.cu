@@ -608,6 +608,7 @@ size_t ibp_sets_registry_size(const ibp_set_desc *sets, int32_t nsets, int word_
 ibp_status ibp_sets_register(const ibp_set_desc *sets, int32_t nsets, int word_bytes,
                              void *registry, size_t registry_bytes_, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_sets_register");
     IBP_ARG(sets && nsets > 0, "sets_register: no sets");
     IBP_ARG(word_bytes == 4 || word_bytes == 8, "sets_register: word size must be 4 or 8 bytes");
     IBP_ARG(registry, "sets_register: null registry");
@@ -633,6 +634,7 @@ ibp_status ibp_batch_fetch(const void *registry, const ibp_request *requests,
                            const int32_t *num_requests, int32_t max_requests, void *workspace,
                            size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_batch_fetch");
     IBP_ARG(registry && requests && num_requests, "batch_fetch: null registry/requests/count");
     IBP_ARG(max_requests > 0 && max_requests <= 8192, "batch_fetch: max_requests must be 1..8192");
     if (!workspace || workspace_bytes < kStatusBytes) {
@@ -662,6 +664,7 @@ ibp_status ibp_batch_autotune(const void *registry, const ibp_request *requests,
                               void *workspace, size_t workspace_bytes, int32_t *chosen,
                               ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_batch_autotune");
     // warm up (and read the header) through the normal entry point
     IBP_RET(ibp_batch_fetch(registry, requests, num_requests, max_requests, workspace,
                             workspace_bytes, stream));
@@ -728,6 +731,7 @@ ibp_status ibp_batch_fetch_sorted(const void *registry, const ibp_request *reque
                                   int32_t num_requests, int64_t total_rows, void *workspace,
                                   size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_batch_fetch_sorted");
     IBP_ARG(registry && requests, "batch_fetch_sorted: null argument");
     IBP_ARG(num_requests > 0 && num_requests <= 8192,
             "batch_fetch_sorted: num_requests must be 1..8192");

@@ -229,6 +229,7 @@ ibp_status ibp_preprocess(const void *dataset, int64_t num_vecs, int64_t vec_siz
                           int word_bytes, float threshold, void *mask, void *bitval,
                           void *workspace, size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_preprocess");
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, false, "preprocess"));
     IBP_ARG((mask && bitval) || vec_size == 0, "preprocess: null mask/bitval");
     IBP_ACCESSIBLE(mask, "preprocess", "mask");
@@ -267,6 +268,7 @@ ibp_status ibp_preprocess_kmeans(const void *dataset, int64_t num_vecs, int64_t 
                                  int32_t *clusters, void *workspace, size_t workspace_bytes,
                                  ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_preprocess_kmeans");
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, true, "preprocess_kmeans"));
     IBP_ARG(num_clusters > 0, "preprocess_kmeans: num_clusters must be positive");
     IBP_ARG(masks && bitvals && (clusters || num_vecs == 0), "preprocess_kmeans: null output");
@@ -308,6 +310,7 @@ ibp_status ibp_get_compress_size(const void *dataset, int64_t num_vecs, int64_t 
                                  const int64_t *index, int64_t num_index, int64_t *sizes,
                                  int64_t *total, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_get_compress_size");
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, false, "get_compress_size"));
     if (num_index < 0) index = nullptr;
     const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
@@ -353,6 +356,7 @@ ibp_status ibp_compress_inplace(void *dataset, int64_t num_vecs, int64_t vec_siz
                                 const int64_t *index, int64_t num_index, int32_t *bitmask,
                                 void *workspace, size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_compress_inplace");
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, true, "compress_inplace"));
     if (num_index < 0) index = nullptr;
     const bool has_index = num_index >= 0;
@@ -387,6 +391,7 @@ size_t ibp_condensed_offsets_workspace_size(int64_t nrows) {
 ibp_status ibp_condensed_offsets(int64_t *sizes_to_offsets, int64_t nrows, int64_t *total,
                                  void *workspace, size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_condensed_offsets");
     IBP_ARG(nrows >= 0, "condensed_offsets: negative row count");
     IBP_ARG(sizes_to_offsets || nrows == 0, "condensed_offsets: null sizes");
     return inclusive_offsets_impl(sizes_to_offsets, nrows, total, workspace, workspace_bytes,
@@ -404,6 +409,7 @@ ibp_status ibp_compress_condensed(const void *dataset, int64_t num_vecs, int64_t
                                   const int64_t *offsets, void *out, void *workspace,
                                   size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_compress_condensed");
     IBP_RET(check_rows(dataset, num_vecs, vec_size, word_bytes, true, "compress_condensed"));
     if (num_index < 0) index = nullptr;
     const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
@@ -454,6 +460,7 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                 int32_t nthreads, int32_t impl, void *workspace,
                                 size_t workspace_bytes, ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_decompress_fetch");
     IBP_RET(check_rows(comp, num_vecs, vec_size, word_bytes, true, "decompress_fetch"));
     if (num_index < 0) index = nullptr;
     const int64_t nrows = num_index >= 0 ? num_index : num_vecs;
@@ -494,6 +501,7 @@ ibp_status ibp_decompress_fetch_condensed(const void *comp, int64_t comp_words,
                                           void *workspace, size_t workspace_bytes,
                                           ibp_stream_t stream) {
     clear_error();
+    IBP_RANGE("ibp_decompress_fetch_condensed");
     IBP_ARG(num_vecs >= 0 && vec_size >= 0 && comp_words >= 0,
             "decompress_fetch_condensed: negative shape");
     IBP_ARG(word_bytes == 4 || word_bytes == 8,

@@ -2,6 +2,7 @@
 // workspace carving and launch geometry.  Everything here is internal to libibp_b200.so.
 #pragma once
 
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -21,6 +22,15 @@ extern std::atomic<unsigned long long> g_launches;  // engine kernels launched s
 
 // Optional CUDA events around row-fetch kernel launches (benchmark profiling hook):
 // profile_begin returns a slot (or -1 when profiling is off or full), profile_end closes it.
+// NVTX range around an entry point (visible in Nsight timelines; near-free without a tool).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define IBP_RANGE(name) ::ibp200::NvtxRange ibp_nvtx_range_(name)
+
 int profile_begin(cudaStream_t st);
 int fetch_dedup_mode();  // ibp_set_fetch_dedup: 0 auto, 1 sort, 2 hash
 void profile_end(int slot, cudaStream_t st);

@@ -463,6 +463,30 @@ ibp_status ibp_server_wait(ibp_server *srv, int64_t id, int32_t timeout_ms, void
     return IBP_OK;
 }
 
+// Withdraw a request that is still queued (not yet admitted to a batch): it will not be
+// fetched, and waiting for it afterwards reports an unknown request.  IBP_ERR_ARGUMENT for an
+// unknown id; IBP_ERR_UNSUPPORTED once the request is admitted (wait for it and release it).
+ibp_status ibp_server_cancel(ibp_server *srv, int64_t id) {
+    clear_error();
+    Server *s = reinterpret_cast<Server *>(srv);
+    IBP_ARG(s, "server_cancel: null server");
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        auto it = s->reqs.find(id);
+        IBP_ARG(it != s->reqs.end(), "server_cancel: unknown request %lld", (long long)id);
+        if (it->second.out_off >= 0) {
+            set_error("server_cancel: request %lld is already admitted", (long long)id);
+            return IBP_ERR_UNSUPPORTED;
+        }
+        auto p = std::find(s->pending.begin(), s->pending.end(), id);
+        if (p != s->pending.end()) s->pending.erase(p);
+        s->reqs.erase(it);
+    }
+    s->cv.notify_all();
+    s->done_cv.notify_all();
+    return IBP_OK;
+}
+
 // Return a finished request's output rows to the arena.
 ibp_status ibp_server_release(ibp_server *srv, int64_t id) {
     clear_error();

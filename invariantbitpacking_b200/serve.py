@@ -67,6 +67,11 @@ class Server:
         rows = self.arena[off:off + nbytes].view(self.reg.dtype).view(count, v)
         return rows, [times[0], times[1], times[2]]
 
+    def cancel(self, rid):
+        """Withdraw a request still waiting for admission (RuntimeError once admitted)."""
+        _capi.check(_lib.ibp_server_cancel(self.handle, int(rid)))
+        self.counts.pop(rid, None)
+
     def release(self, rid):
         _capi.check(_lib.ibp_server_release(self.handle, int(rid)))
         self.counts.pop(rid, None)

@@ -91,3 +91,44 @@ def test_server_results_equal_solo_fetches(ibp, limits):
         assert st["batches"] >= sum(r[3] * sets[r[0]][0].shape[1] * 8 for r in reqs) // (
             limits[1] + big)
     srv.close()
+
+
+def test_server_cancel_and_admission_wait(ibp):
+    """A request that cannot be admitted (its output does not fit the arena beside an
+    unreleased one) stays queued and can be withdrawn; an admitted one cannot; the server
+    keeps serving afterwards."""
+    from invariantbitpacking_b200.batch import SetRegistry
+    from invariantbitpacking_b200.serve import Server
+    rng = np.random.default_rng(9)
+    n, v = 4000, 64
+    f = rng.normal(0, 0.3, (n, 2 * v)).astype(np.float32)
+    f = (f.view(np.uint32) & np.uint32(0xFFFF8000)).view(np.float32)
+    d = np.ascontiguousarray(f).view(np.int64)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    cl = ibp.get_single_compress_len(x, m, b)
+    bm = ibp.compress_inplace(x, m, b)
+    reg = SetRegistry([(x, m, b, bm, cl)])
+    rows = 3000
+    srv = Server(reg, arena_bytes=rows * v * 8 + 4096, index_capacity=1 << 16, max_batch=4)
+    ra = rng.integers(0, n, rows)
+    a = srv.submit(0, ra)
+    out_a, _ = srv.wait(a, 20000)             # admitted and done; its rows hold the arena
+    b_id = srv.submit(0, rng.integers(0, n, rows))
+    import time
+    time.sleep(0.05)
+    assert srv.stats()["pending"] == 1        # cannot fit until `a` is released
+    srv.cancel(b_id)
+    assert srv.stats()["pending"] == 0
+    with pytest.raises(RuntimeError):
+        srv.cancel(a)                          # already admitted
+    with pytest.raises(RuntimeError):
+        srv.wait(b_id, 100)                    # withdrawn: unknown now
+    assert np.array_equal(out_a.cpu().numpy(), d[ra])
+    srv.release(a)
+    rc = rng.integers(0, n, 100)
+    c = srv.submit(0, rc)
+    out_c, _ = srv.wait(c, 20000)
+    assert np.array_equal(out_c.cpu().numpy(), d[rc])
+    srv.release(c)
+    srv.close()
