@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--shard", action="store_true",
                     help="graph_features under torchrun: split every batch across the ranks "
                          "(strong scaling) instead of one replica per rank")
+    ap.add_argument("--inflight", type=int, default=4,
+                    help="served_mix: batches the server keeps on the GPU")
     ap.add_argument("--batch-mb", type=int, default=128,
                     help="served_mix: output MiB one server batch admits")
     return ap.parse_args()
@@ -789,8 +791,8 @@ def served_sets(torch, ibp):
 def run_served(args):
     """Poisson request streams over 8 sets; requests of log-uniform [256, 262144] rows with
     uniform row numbers; the continuous-batching server (40 GB output arena) against one
-    plain decompress_fetch per request in arrival order.  Latency = completion time minus
-    scheduled arrival time."""
+    plain decompress_fetch per request in arrival order, ours and (when its build is present)
+    the reference's.  Latency = completion time minus scheduled arrival time."""
     import threading
     import torch
     torch.cuda.set_device(0)
@@ -802,7 +804,14 @@ def run_served(args):
     setup_s = time.perf_counter() - t0
     reg = SetRegistry(sets)
     srv = Server(reg, arena_bytes=40 << 30, index_capacity=1 << 26, max_batch=256,
-                 max_inflight=2, batch_bytes=args.batch_mb << 20)
+                 max_inflight=args.inflight, batch_bytes=args.batch_mb << 20)
+    import glob
+    ref = None
+    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    if mods:  # the reference's decompress_fetch, built from its sources, as a third arm
+        sys.path.insert(0, os.path.dirname(mods[0]))
+        import ibp_cuda as ref
+        ref.print_debug(False)
     rates = [float(r) for r in args.rates.split(",")]
     nreq = args.requests
     rng = np.random.default_rng(7)
@@ -864,44 +873,56 @@ def run_served(args):
                   "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
                   "GBps": round(total_bytes / (t_last - base) / 1e9, 3)}
 
-        # ---- per request: one plain decompress_fetch per request, in arrival order
+        # ---- per request: one plain decompress_fetch per request, in arrival order (ours,
+        # and the reference's own when its build is present)
         rows_pin = [torch.from_numpy(r).pin_memory() for r in rows]
-        evs = [None] * nreq
-        done_t = [0.0] * nreq
-        base2 = time.monotonic() + 0.05
 
-        def reaper():
+        def per_request(fetch):
+            evs = [None] * nreq
+            done_t = [0.0] * nreq
+            base2 = time.monotonic() + 0.05
+
+            def reaper():
+                for j in range(nreq):
+                    while evs[j] is None:
+                        time.sleep(0.00005)
+                    evs[j].synchronize()
+                    done_t[j] = time.monotonic()
+
+            rt = threading.Thread(target=reaper)
+            rt.start()
+            outs = [None] * nreq
             for j in range(nreq):
-                while evs[j] is None:
-                    time.sleep(0.00005)
-                evs[j].synchronize()
-                done_t[j] = time.monotonic()
+                t = base2 + arrive[j]
+                while time.monotonic() < t:
+                    pass
+                x, m, b, bm, cl = sets[sids[j]]
+                idx = rows_pin[j].to("cuda", non_blocking=True)
+                outs[j] = fetch(x, m, b, bm, cl, idx)
+                ev = torch.cuda.Event()
+                ev.record()
+                evs[j] = ev
+                if j >= 2:
+                    outs[j - 2] = None  # let the caching allocator reuse finished outputs
+            rt.join()
+            lat2 = [done_t[j] - (base2 + arrive[j]) for j in range(nreq)]
+            del outs
+            torch.cuda.empty_cache()
+            return {"p50_ms": round(float(np.percentile(lat2, 50)) * 1e3, 3),
+                    "p99_ms": round(float(np.percentile(lat2, 99)) * 1e3, 3),
+                    "GBps": round(total_bytes / (max(done_t) - base2) / 1e9, 3)}
 
-        rt = threading.Thread(target=reaper)
-        rt.start()
-        outs = [None] * nreq
-        for j in range(nreq):
-            t = base2 + arrive[j]
-            while time.monotonic() < t:
-                pass
-            x, m, b, bm, cl = sets[sids[j]]
-            idx = rows_pin[j].to("cuda", non_blocking=True)
-            outs[j] = ibp.decompress_fetch(x, m, b, bm, torch.device("cuda"), cl, idx)
-            ev = torch.cuda.Event()
-            ev.record()
-            evs[j] = ev
-            if j >= 2:
-                outs[j - 2] = None  # let the caching allocator reuse finished outputs
-        rt.join()
-        lat2 = [done_t[j] - (base2 + arrive[j]) for j in range(nreq)]
-        plain = {"p50_ms": round(float(np.percentile(lat2, 50)) * 1e3, 3),
-                 "p99_ms": round(float(np.percentile(lat2, 99)) * 1e3, 3),
-                 "GBps": round(total_bytes / (max(done_t) - base2) / 1e9, 3)}
-        del outs
-        torch.cuda.empty_cache()
-        results.append({"rate_per_s": rate, "requests": nreq,
-                        "output_GB": round(total_bytes / 1e9, 2), "served": served,
-                        "per_request": plain})
+        dev = torch.device("cuda")
+        plain = per_request(lambda x, m, b, bm, cl, idx:
+                            ibp.decompress_fetch(x, m, b, bm, dev, cl, idx))
+        entry = {"rate_per_s": rate, "requests": nreq,
+                 "output_GB": round(total_bytes / 1e9, 2), "served": served,
+                 "per_request": plain}
+        if ref is not None:
+            entry["per_request_reference"] = per_request(
+                lambda x, m, b, bm, cl, idx:
+                ref.decompress_fetch(x, m, b, bm, dev, cl, idx, None, None, None, None))
+        results.append(entry)
     st = srv.stats()
     srv.close()
     head = results[0]
@@ -913,7 +934,7 @@ def run_served(args):
         "dtype": "int64", "data": "synthetic",
         "config": {"workload": "served_mix: 8 pinned sets (~384 MB each), V in {64,128,256,512}, "
                                "Poisson arrivals, log-uniform [256, 262144] rows per request",
-                   "arena_GB": 40, "max_batch": 256, "max_inflight": 2,
+                   "arena_GB": 40, "max_batch": 256, "max_inflight": args.inflight,
                    "batch_MiB": args.batch_mb,
                    "setup_s": round(setup_s, 1), "batches": st["batches"],
                    "bit_exact_checked_requests": checked},
