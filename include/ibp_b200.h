@@ -76,7 +76,9 @@ unsigned long long ibp_kernel_launch_count(void);
 /* Device status word of the last call that used `workspace`: bit 0 = an index was out of
  * range; bit 1 = a row marked compressed has a bitmap whose stream would not fit the row
  * (the bitmask/mask do not belong to the data), and its output row was left untouched;
- * bit 2 = a sorted batch's request counts did not add up to its stated total_rows.
+ * bit 2 = a sorted batch's request counts did not add up to its stated total_rows;
+ * bit 3 = a repeated index gave up waiting (2^20 polls, a fraction of a second) for the row
+ * of its first occurrence, and its output row was left untouched.
  * Enqueues a copy on `stream` and waits for it (blocking). */
 ibp_status ibp_read_status(const void *workspace, int32_t *status, ibp_stream_t stream);
 

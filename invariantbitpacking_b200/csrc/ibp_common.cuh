@@ -80,6 +80,7 @@ constexpr size_t kStatusBytes = 256;    // head of every workspace: device statu
 constexpr int32_t kStatusBadIndex = 1;    // bit 0: an index was out of range
 constexpr int32_t kStatusCorruptRow = 2;  // bit 1: a row's bitmap does not fit its mask
 constexpr int32_t kStatusBadTable = 4;    // bit 2: request counts disagree with a stated total
+constexpr int32_t kStatusWaitTimeout = 8;  // bit 3: a repeat gave up waiting for its first row
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

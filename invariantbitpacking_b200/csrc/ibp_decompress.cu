@@ -26,8 +26,10 @@
 //    read neighbouring host pages.  Fixed-stride compressed rows in HBM, and sparse batches
 //    of them in host memory, where order gains little, claim rows in an open-addressing
 //    hash table instead: inside the fetch for host rows (hidden behind PCIe), in a claim
-//    pass that lists the distinct rows for HBM rows.  Repeats are filled afterwards by a
-//    copy kernel (Zipf mini-batches repeat hot rows a lot).
+//    pass that lists the distinct rows for HBM rows.  Repeats (Zipf mini-batches repeat hot
+//    rows a lot) copy their first occurrence's output row: inside the fetch for host rows,
+//    once that row is published in the table (so the copies overlap the PCIe reads), and
+//    in a copy kernel afterwards for the other modes.
 //  * no allocation, no host synchronisation: everything lives in the caller's workspace
 //    and is enqueued on the caller's stream.
 #include <cub/device/device_radix_sort.cuh>
@@ -59,7 +61,9 @@ struct FetchArgs {
     int gmax;             // largest chunk a warp takes (positions); 0: its row slots
     bool async_rows;      // rows in device memory: first reads as asynchronous copies
     int64_t *hkeys;       // in-fetch claims: open-addressing table of rows (-1 = empty) ...
-    int64_t *hpos;        // ... and the position that claimed each (nullptr: no claims)
+    int64_t *hpos;        // ... and, once its row is written, the position that claimed each
+                          // with kRowDone set (-1 before; nullptr: no claims); repeats are
+                          // copied inside the fetch
     int64_t hslots;       // the table's slots
     const int64_t *list;  // positions to fetch (claimed heads), or nullptr: all positions
     const unsigned long long *list_len;  // entries of `list` (device)
@@ -72,26 +76,102 @@ __device__ __forceinline__ uint64_t row_hash(int64_t key, int64_t slots) {
     return __umul64hi((uint64_t)key * 0x9E3779B97F4A7C15ull, (uint64_t)slots);
 }
 
-__device__ __forceinline__ bool hash_claim(int64_t *keys, int64_t *pos, int64_t slots,
-                                           int64_t key, int64_t k) {
+// The table slot holding `key` after this call: claimed by it (`won`) or by an earlier one;
+// -1 when the table is full (it never is: it has twice as many slots as positions).
+__device__ __forceinline__ int64_t hash_claim_slot(int64_t *keys, int64_t slots, int64_t key,
+                                                   bool &won) {
+    won = false;
     uint64_t h = row_hash(key, slots);
     for (int64_t probe = 0; probe < slots; ++probe) {
         // a plain read first: a row already claimed (hot rows of a skewed batch) costs no
         // atomic, so repeats do not queue on one address
         const int64_t cur = *reinterpret_cast<volatile int64_t *>(keys + h);
-        if (cur == key) return false;
+        if (cur == key) return (int64_t)h;
         if (cur == -1) {
             const unsigned long long old = atomicCAS(
                 reinterpret_cast<unsigned long long *>(keys + h), ~0ull, (unsigned long long)key);
             if (old == ~0ull) {
-                pos[h] = k;
-                return true;
+                won = true;
+                return (int64_t)h;
             }
-            if ((int64_t)old == key) return false;
+            if ((int64_t)old == key) return (int64_t)h;
         }
         h = h + 1 == (uint64_t)slots ? 0 : h + 1;
     }
-    return false;
+    return -1;
+}
+
+__device__ __forceinline__ bool hash_claim(int64_t *keys, int64_t *pos, int64_t slots,
+                                           int64_t key, int64_t k) {
+    bool won;
+    const int64_t h = hash_claim_slot(keys, slots, key, won);
+    if (won) pos[h] = k;
+    return won;
+}
+
+// In-fetch claims publish each claimed row's position with this bit once the row is written.
+constexpr int64_t kRowDone = 1ll << 62;
+constexpr int kRepeatWaitLimit = 1 << 20;  // polls (~0.25 us apart) before a repeat gives up
+
+__device__ __forceinline__ int64_t load_acquire(const int64_t *p) {
+    int64_t x;
+    asm volatile("ld.acquire.gpu.global.s64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
+    return x;
+}
+
+__device__ __forceinline__ void store_release(int64_t *p, int64_t x) {
+    asm volatile("st.release.gpu.global.s64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
+}
+
+// Copy rows src -> dst for the lanes of `dm` (each lane's src/dst), four rows at a time: all
+// four rows' loads before any store (16-byte moves when the rows are aligned), so the loads'
+// latencies overlap.  Sources are read through L2 (other SMs may have just written them).
+template <typename U>
+__device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_row, int64_t v,
+                                          bool vec_rows) {
+    constexpr int R = 4;
+    const int lane = threadIdx.x & 31;
+    while (dm) {
+        const U *src[R];
+        U *dst[R];
+        int cnt = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            src[r] = src_row;
+            dst[r] = dst_row;
+            if (dm) {
+                const int j = __ffs(dm) - 1;
+                dm &= dm - 1;
+                src[r] = reinterpret_cast<const U *>(__shfl_sync(
+                    0xffffffffu, reinterpret_cast<unsigned long long>(src_row), j));
+                dst[r] = reinterpret_cast<U *>(__shfl_sync(
+                    0xffffffffu, reinterpret_cast<unsigned long long>(dst_row), j));
+                cnt = r + 1;
+            }
+        }
+        if (vec_rows) {
+            const int64_t n16 = v * (int64_t)sizeof(U) / 16;
+            for (int64_t q = lane; q < n16; q += 32) {
+                uint4 t[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) t[r] = __ldcg(reinterpret_cast<const uint4 *>(src[r]) + q);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
+            }
+        } else {
+            for (int64_t q = lane; q < v; q += 32) {
+                U t[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) t[r] = __ldcg(src[r] + q);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) dst[r][q] = t[r];
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
@@ -146,66 +226,26 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
     }
 }
 
-// Repeats of a hashed fetch: each position whose row another position claimed copies that
-// position's output row.  A warp copies the repeats among its 32 positions four rows at a
-// time (all four rows' loads before any store, 16-byte moves when the rows are aligned), so
-// the copies' load latencies overlap.
+// Repeats of a hashed fetch whose claims came from claim_heads_kernel: each position whose
+// row another position claimed copies that position's output row (copy_rows, four rows at
+// a time per warp).
 template <typename U>
 __global__ void __launch_bounds__(256)
 fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
                    const int64_t *__restrict__ hkeys, const int64_t *__restrict__ hpos,
                    int64_t hslots, U *__restrict__ out, int64_t v) {
-    constexpr int R = 4;
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int64_t bytes = v * (int64_t)sizeof(U);
-    const bool vec_rows = (bytes & 15) == 0 && (((uintptr_t)out) & 15) == 0;
+    const bool vec_rows = ((v * (int64_t)sizeof(U)) & 15) == 0 && (((uintptr_t)out) & 15) == 0;
     for (int64_t k0 = warp * 32; k0 < nrows; k0 += nwarps * 32) {
         const int64_t k = k0 + lane;
         const int64_t key = k < nrows ? idx[k] : -1;
         int64_t hp = -1;
         if (key >= 0 && key < n) hp = hash_find(hkeys, hpos, hslots, key);
-        unsigned dm = __ballot_sync(0xffffffffu, hp >= 0 && hp != k);
-        while (dm) {
-            const U *src[R];
-            U *dst[R];
-            int cnt = 0;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                src[r] = out;
-                dst[r] = out;
-                if (dm) {
-                    const int j = __ffs(dm) - 1;
-                    dm &= dm - 1;
-                    src[r] = out + __shfl_sync(0xffffffffu, hp, j) * v;
-                    dst[r] = out + (k0 + j) * v;
-                    cnt = r + 1;
-                }
-            }
-            if (vec_rows) {
-                const int64_t n16 = bytes / 16;
-                for (int64_t q = lane; q < n16; q += 32) {
-                    uint4 t[R];
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (r < cnt) t[r] = reinterpret_cast<const uint4 *>(src[r])[q];
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
-                }
-            } else {
-                for (int64_t q = lane; q < v; q += 32) {
-                    U t[R];
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (r < cnt) t[r] = src[r][q];
-#pragma unroll
-                    for (int r = 0; r < R; ++r)
-                        if (r < cnt) dst[r][q] = t[r];
-                }
-            }
-        }
+        const bool rep = hp >= 0 && hp != k;
+        copy_rows<U>(__ballot_sync(0xffffffffu, rep), out + (rep ? hp : 0) * v,
+                     out + (rep ? k : 0) * v, v, vec_rows);
     }
 }
 
@@ -216,9 +256,15 @@ fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
 template <typename U, int NC, bool EXACT, bool ASYNC>
 __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr bool kClaims = !EXACT && !ASYNC;  // in-fetch claims: fixed-stride host rows
     const int lane = threadIdx.x & 31;
     U *slots = reinterpret_cast<U *>(smem) +
                (int64_t)(threadIdx.x >> 5) * a.slots * (ASYNC ? 2 : 1) * a.slot_words;
+    // in-fetch claims: 64 words per warp after all the row slots
+    int64_t *claim = reinterpret_cast<int64_t *>(
+                         reinterpret_cast<U *>(smem) + (int64_t)(blockDim.x >> 5) * a.slots *
+                                                           (ASYNC ? 2 : 1) * a.slot_words) +
+                     (threadIdx.x >> 5) * 64;
     LaneTables<U, NC> lt;
     if (!a.raw_only) lt.load(a.s.t, a.s.v);
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -249,13 +295,25 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         const bool bad = head && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         head = head && !bad;
-        if (a.hkeys) {
-            // one claim per distinct row of the chunk (its lowest lane)
+        // in-fetch claims: one claim per distinct row of the chunk (its lowest lane); the
+        // other lanes of that row, and the lanes whose row was claimed earlier, are repeats.
+        // Each lane parks its table slot (kRowDone set: it claimed the row) and position in
+        // shared memory until its chunk's rows are fetched, which keeps them out of the
+        // registers the fetch needs.
+        bool rep = false;
+        if (kClaims && a.hkeys) {
             const unsigned same = __match_any_sync(0xffffffffu, head ? key : (int64_t)-1);
-            head = head && (__ffs(same) - 1) == lane &&
-                   hash_claim(a.hkeys, a.hpos, a.hslots, key, k);
+            const int first = __ffs(same) - 1;
+            bool won = false;
+            int64_t slot = -1;
+            if (head && first == lane) slot = hash_claim_slot(a.hkeys, a.hslots, key, won);
+            slot = __shfl_sync(0xffffffffu, slot, first);
+            rep = head && !won && slot >= 0;
+            head = won;
+            claim[lane] = head ? slot | kRowDone : (rep ? slot : -1);
+            claim[32 + lane] = k;
         }
-        U *orow = a.out + (head ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
+        U *orow = a.out + (head || rep ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
         if constexpr (EXACT) {
             fetch_heads_exact<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
                                      a.status);
@@ -268,6 +326,44 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
             else
                 fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
                                    packed, a.status);
+        }
+        if (kClaims && a.hkeys) {
+            // publish this chunk's rows (every lane's stores are ordered before the release
+            // by the warp barrier), then copy its repeats once their rows are published.  A
+            // warp waits only after publishing all of its own claims, so every row waited
+            // on belongs to a warp that is still fetching and waits on nothing.
+            __syncwarp();
+            const int64_t cw = claim[lane];
+            const int64_t kk = claim[32 + lane];
+            const bool own = cw >= 0 && (cw & kRowDone);
+            const bool rep = cw >= 0 && !own;
+            const int64_t slot = cw & ~kRowDone;
+            if (own) store_release(a.hpos + slot, kk | kRowDone);
+            if (__any_sync(0xffffffffu, rep)) {
+                int64_t src = -1;
+                // once any wait has given up, later ones make a single check
+                const int limit =
+                    (*reinterpret_cast<volatile int32_t *>(a.status) & kStatusWaitTimeout)
+                        ? 0
+                        : kRepeatWaitLimit;
+                for (int it = 0;; ++it) {
+                    if (rep && src < 0) {
+                        const int64_t hv = load_acquire(a.hpos + slot);
+                        if (hv >= 0 && (hv & kRowDone)) src = hv & ~kRowDone;
+                    }
+                    if (__all_sync(0xffffffffu, !rep || src >= 0)) break;
+                    if (it >= limit) {
+                        if (rep && src < 0) atomicOr(a.status, kStatusWaitTimeout);
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                const bool go = rep && src >= 0;
+                copy_rows<U>(__ballot_sync(0xffffffffu, go), a.out + (go ? src : 0) * a.s.v,
+                             a.out + (go ? kk : 0) * a.s.v, a.s.v,
+                             ((a.s.v * (int64_t)sizeof(U)) & 15) == 0 &&
+                                 (((uintptr_t)a.out) & 15) == 0);
+            }
         }
     }
 }
@@ -346,10 +442,13 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     const int maxs = device_max_smem_optin();
     // row slots per warp: up to kRowsInFlight within ~96 KB per block; long rows get fewer
     // slots and then fewer warps
+    // (plus 512 bytes per warp for the in-fetch claims' slots and positions)
+    const size_t warp_extra = a.hkeys ? 64 * sizeof(int64_t) : 0;
+    auto smem_of = [&](int s, int t) { return (slot_bytes * s + warp_extra) * (t / 32); };
     int slots = kRowsInFlight;
-    while (slots > 1 && slot_bytes * slots * (threads / 32) > 96 * 1024) --slots;
-    while (threads > 32 && slot_bytes * slots * (threads / 32) > (size_t)maxs) threads -= 32;
-    const size_t smem = slot_bytes * slots * (threads / 32);
+    while (slots > 1 && smem_of(slots, threads) > 96 * 1024) --slots;
+    while (threads > 32 && smem_of(slots, threads) > (size_t)maxs) threads -= 32;
+    const size_t smem = smem_of(slots, threads);
     if ((int64_t)smem > maxs) {
         set_error("rows of %lld words do not fit the fetch kernel's shared-memory slot",
                   (long long)a.s.v);
@@ -477,7 +576,8 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         int64_t *hkeys = c.take<int64_t>(slots);
         int64_t *hpos = c.take<int64_t>(slots);
         int64_t *heads = c.take<int64_t>(nidx);
-        IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, sizeof(int64_t) * slots, st));
+        // keys -1 (empty); positions -1 (unpublished) for the in-fetch claims
+        IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, (char *)(hpos + slots) - (char *)hkeys, st));
         a.keys = idx;
         if (on_device) {
             // HBM rows: claim in a pass of its own, so the fetch walks distinct rows only, 32
@@ -492,10 +592,12 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
             a.list = heads;
             a.list_len = nheads;
         } else {
-            // host rows: claims happen inside the fetch, hidden behind its PCIe reads
+            // host rows: claims and repeat copies happen inside the fetch, hidden behind its
+            // PCIe reads
             a.hkeys = hkeys;
             a.hpos = hpos;
             a.hslots = slots;
+            return launch_fetch<U>(a, nblks, nthreads, st);
         }
         IBP_RET(launch_fetch<U>(a, nblks, nthreads, st));
         const int64_t fb = std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);

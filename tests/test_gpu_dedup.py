@@ -74,3 +74,50 @@ def test_dedup_modes_condensed(ibp, mode):
         out = ibp.decompress_fetch_condensed(comp, offs.cuda(), m, b, v, "cuda",
                                              torch.from_numpy(idx).cuda())
         assert np.array_equal(out.cpu().numpy(), d[idx])
+
+
+@pytest.mark.parametrize("pattern", ["zipf", "one_row", "pairs"])
+@pytest.mark.parametrize("aligned", [True, False], ids=["out16", "out8"])
+def test_in_fetch_repeats(ibp, oracle, pattern, aligned):
+    """Host rows under hash claims: each repeat copies its first occurrence's output row
+    inside the fetch, once that row is published in the table.  Every row must be exact, into
+    16-byte aligned and unaligned outputs, and no wait may give up (status bit 3)."""
+    import ctypes
+    from invariantbitpacking_b200 import _capi
+    lib = _capi.lib
+    rng = np.random.default_rng(77)
+    n, v = 30000, 64
+    d = make(rng, n, v, 8)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    bm = ibp.compress_inplace(x, m, b)
+    cl = ibp.get_single_compress_len(x, m, b)
+    torch.cuda.synchronize()
+    comp = x.numpy().copy()
+    if pattern == "zipf":
+        idx = np.minimum(rng.zipf(1.1, 120000) - 1, n - 1)
+    elif pattern == "one_row":
+        idx = np.full(50000, 1234)
+    else:  # each row twice, the two occurrences next to each other or far apart
+        r = rng.permutation(n)[:20000]
+        idx = np.concatenate([np.repeat(r[:10000], 2), r[10000:], r[10000:][::-1]])
+    idx = idx.astype(np.int64)
+    ti = torch.from_numpy(idx).cuda()
+    nidx = idx.size
+    buf = torch.full((nidx * v + 1,), 7, dtype=torch.int64, device="cuda")
+    out = buf[:nidx * v] if aligned else buf[1:]
+    wsb = lib.ibp_decompress_fetch_workspace_size(nidx, v, 8, 1)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _capi.check(lib.ibp_set_fetch_dedup(2))
+    try:
+        _capi.check(lib.ibp_decompress_fetch(x.data_ptr(), n, v, 8, m.data_ptr(), b.data_ptr(),
+                                             bm.data_ptr(), ti.data_ptr(), nidx, cl,
+                                             out.data_ptr(), -1, -1, -1, ws.data_ptr(), wsb, st))
+        status = ctypes.c_int32(-1)
+        _capi.check(lib.ibp_read_status(ws.data_ptr(), ctypes.byref(status), st))
+    finally:
+        _capi.check(lib.ibp_set_fetch_dedup(0))
+    assert status.value == 0
+    want = oracle.decompress(comp, m.cpu().numpy(), b.cpu().numpy(), bm.cpu().numpy(), idx)
+    assert np.array_equal(out.view(nidx, v).cpu().numpy(), want)
