@@ -341,11 +341,14 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
             if (own) store_release(a.hpos + slot, kk | kRowDone);
             if (__any_sync(0xffffffffu, rep)) {
                 int64_t src = -1;
-                // once any wait has given up, later ones make a single check
-                const int limit =
-                    (*reinterpret_cast<volatile int32_t *>(a.status) & kStatusWaitTimeout)
-                        ? 0
-                        : kRepeatWaitLimit;
+                // once any wait has given up, later ones make a single check (lane 0 reads
+                // the status word, so that every lane has the same bound)
+                int limit = 0;
+                if (lane == 0)
+                    limit = (*reinterpret_cast<volatile int32_t *>(a.status) & kStatusWaitTimeout)
+                                ? 0
+                                : kRepeatWaitLimit;
+                limit = __shfl_sync(0xffffffffu, limit, 0);
                 for (int it = 0;; ++it) {
                     if (rep && src < 0) {
                         const int64_t hv = load_acquire(a.hpos + slot);

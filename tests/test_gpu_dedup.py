@@ -78,10 +78,12 @@ def test_dedup_modes_condensed(ibp, mode):
 
 @pytest.mark.parametrize("pattern", ["zipf", "one_row", "pairs"])
 @pytest.mark.parametrize("aligned", [True, False], ids=["out16", "out8"])
-def test_in_fetch_repeats(ibp, oracle, pattern, aligned):
-    """Host rows under hash claims: each repeat copies its first occurrence's output row
-    inside the fetch, once that row is published in the table.  Every row must be exact, into
-    16-byte aligned and unaligned outputs, and no wait may give up (status bit 3)."""
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where):
+    """Hash claims (made inside the fetch for host rows, by a claim pass for device rows):
+    each repeat copies its first occurrence's output row inside the fetch, once that row is
+    published in the table.  Every row must be exact, into 16-byte aligned and unaligned
+    outputs, and no wait may give up (status bit 3)."""
     import ctypes
     from invariantbitpacking_b200 import _capi
     lib = _capi.lib
@@ -102,6 +104,8 @@ def test_in_fetch_repeats(ibp, oracle, pattern, aligned):
         r = rng.permutation(n)[:20000]
         idx = np.concatenate([np.repeat(r[:10000], 2), r[10000:], r[10000:][::-1]])
     idx = idx.astype(np.int64)
+    if where == "device":
+        x = x.cuda()
     ti = torch.from_numpy(idx).cuda()
     nidx = idx.size
     buf = torch.full((nidx * v + 1,), 7, dtype=torch.int64, device="cuda")
