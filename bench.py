@@ -228,6 +228,71 @@ def host_gather_copy_baseline(torch, d, batches, seconds=5.0):
             "kind": "uncompressed host gather + H2D copy", "steps": k}
 
 
+def cpu_core_sweep(torch, d, mask, bitval, comp, bitmask, batches, seconds):
+    """The host-side baselines at 1, 8 and all host threads (the reference's cores sweep):
+    the oracle's decompress of mini-batch prefixes, the uncompressed gather (torch
+    index_select into pinned staging, then one H2D copy) of whole mini-batches, and the
+    oracle's compress of the first 200k rows; each sample bounded to about seconds/3."""
+    import oracle
+    allc = os.cpu_count() or 1
+    cores = sorted({1, min(8, allc), allc})
+    each = max(0.5, min(3.0, seconds / 3))
+    dt = torch.from_numpy(d)
+    nmax = max(len(b) for b in batches)
+    stage = torch.empty((nmax, V), dtype=torch.int64)
+    if torch.cuda.is_available():
+        stage = stage.pin_memory()
+    dv = (torch.empty((nmax, V), dtype=torch.int64, device="cuda")
+          if torch.cuda.is_available() else None)
+    tidx = [torch.from_numpy(b) for b in batches]
+    threads0 = torch.get_num_threads()
+
+    def timed(fn):
+        t0 = time.perf_counter()
+        nbytes, k = 0, 0
+        while time.perf_counter() - t0 < each:
+            nbytes += fn(k)
+            k += 1
+        return nbytes / (time.perf_counter() - t0) / 1e9
+
+    def dec(k):
+        idx = batches[k % len(batches)][:50_000]
+        oracle.decompress(comp, mask, bitval, bitmask, idx)
+        return len(idx) * V * 8
+
+    def gather(k):
+        idx = tidx[k % len(tidx)]
+        torch.index_select(dt, 0, idx, out=stage[:len(idx)])
+        if dv is not None:
+            dv[:len(idx)].copy_(stage[:len(idx)], non_blocking=True)
+            torch.cuda.synchronize()
+        return len(idx) * V * 8
+
+    sample = d[:200_000]
+
+    def cmp(k):
+        oracle.compress(sample, mask, bitval)
+        return sample.nbytes
+
+    out = {"unit": "GB/s", "cores_available": allc, "decompress": [], "gather_copy": []}
+    try:
+        for c in cores:
+            oracle.set_threads(c)
+            out["decompress"].append({"cores": c, "value": round(timed(dec), 3)})
+            torch.set_num_threads(c)
+            out["gather_copy"].append({"cores": c, "value": round(timed(gather), 3)})
+        oracle.set_threads(allc)
+        out["compress"] = {"cores": allc, "value": round(timed(cmp), 3),
+                           "sample": "the first 200k rows (102 MB), oracle compress"}
+    finally:
+        torch.set_num_threads(threads0)
+        oracle.set_threads(allc)
+    out["what"] = ("decompress: oracle on 50k-row prefixes of the mini-batches; gather_copy: "
+                   "uncompressed rows of whole mini-batches gathered on the host and copied "
+                   "to the GPU; compress: oracle compress; delivered (uncompressed) GB/s")
+    return out
+
+
 WORKLOAD = ("graph_features: 2.4M x 128 fp32 N(0,0.3^2), 8 mantissa bits, 30% zeros -> "
             "int64 [2.4M x 64], pinned host (1.2 GB)")
 BATCH_DESC = "Zipf(1.1) mini-batches cycling 100k/200k/400k rows"
@@ -1212,6 +1277,11 @@ def main():
         cpu = cpu_baseline(d, m.cpu().numpy(), b.cpu().numpy(), x.numpy(), bm.cpu().numpy(),
                            batches, args.cpu_seconds)
         gather = host_gather_copy_baseline(torch, d, batches)
+        sweep = cpu_core_sweep(torch, d, m.cpu().numpy(), b.cpu().numpy(), x.numpy(),
+                               bm.cpu().numpy(), batches, args.cpu_seconds)
+        if setup and "ours" in setup:
+            sweep["gpu_compress_inplace"] = round(
+                d.nbytes / setup["ours"]["compress_inplace_ms"] / 1e6, 3)
         nrows_avg = rows / args.steps
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": ws,
@@ -1243,6 +1313,7 @@ def main():
             "roofline_hbm": hbm,
             "cpu_baseline": cpu,
             "cpu_baseline_uncompressed_gather": gather,
+            "cpu_core_sweep": sweep,
             "gpu_uncompressed_gather": {"value": round(raw_gbs, 3), "unit": "GB/s",
                                         "what": "same batches, uncompressed pinned rows, "
                                                 "zero-copy gather (impl 2) with the same "

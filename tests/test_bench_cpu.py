@@ -19,3 +19,25 @@ def test_reference_arm_prints_contract_line():
         assert key in line, key
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_cpu_core_sweep_small():
+    """The host-side cores sweep (oracle decompress, uncompressed gather, oracle compress) on a
+    small set: one entry per thread count, positive rates."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    import oracle
+    from invariantbitpacking_b200 import synthetic
+    d = synthetic.graph_features(n=3000)
+    m, b, _ = oracle.preprocess(d, None)
+    comp, bm = oracle.compress(d, m, b)
+    rng = np.random.default_rng(1)
+    batches = [rng.integers(0, 3000, 500), rng.integers(0, 3000, 900)]
+    r = bench.cpu_core_sweep(torch, d, m, b, comp, bm, batches, 1.5)
+    cores = sorted({1, min(8, os.cpu_count() or 1), os.cpu_count() or 1})
+    assert [e["cores"] for e in r["decompress"]] == cores
+    assert [e["cores"] for e in r["gather_copy"]] == cores
+    assert all(e["value"] > 0 for e in r["decompress"] + r["gather_copy"])
+    assert r["compress"]["value"] > 0
