@@ -56,11 +56,12 @@ int ibp_abi_version(void);
 void ibp_set_debug(int on);
 
 /* How decompress_fetch (and its condensed and no-alloc forms) finds the repeated rows of an
- * index array, process-wide: 0 = auto (hash table for fixed-stride compressed rows in device
- * memory, or in host memory when the index has fewer than a quarter as many entries as the
- * set has rows; else sort), 1 = always
- * sort (rows then fetched in row order), 2 = always hash.  No counterpart in the reference
- * (it always sorts). */
+ * index array, process-wide: 0 = auto (hash table for compressed rows, fixed-stride or
+ * condensed, in device memory, or in host memory when the index has fewer than a quarter as
+ * many entries as the set has rows; else sort), 1 = always sort (rows then fetched in row
+ * order), 2 = always hash (repeats are then copied inside the fetch for host rows).  Dense
+ * host batches whose rows repeat a lot (skewed, e.g. Zipf) are faster with 2; dense batches
+ * with few repeats are faster sorted.  No counterpart in the reference (it always sorts). */
 ibp_status ibp_set_fetch_dedup(int32_t mode);
 
 /* Profiling hooks (benchmarks): after ibp_profile_enable(cap), the next `cap` row-fetch

@@ -21,12 +21,12 @@
 //    loaded once per warp; longer rows read them through the L1 cache, four chunks at a
 //    time, and place the bits of columns that keep at most 4 directly from the mask.
 //  * index arrays: each distinct row crosses the link once.  Dense batches of host rows (a
-//    quarter of the rows or more), condensed rows and raw gathers are fetched in sorted
-//    index order (cub radix sort on only the bits the row count needs) so concurrent warps
-//    read neighbouring host pages.  Fixed-stride compressed rows in HBM, and sparse batches
-//    of them in host memory, where order gains little, claim rows in an open-addressing
-//    hash table instead: inside the fetch for host rows (hidden behind PCIe), in a claim
-//    pass that lists the distinct rows for HBM rows.  Repeats (Zipf mini-batches repeat hot
+//    quarter of the rows or more) and raw gathers are fetched in sorted index order (cub
+//    radix sort on only the bits the row count needs) so concurrent warps read neighbouring
+//    host pages.  Compressed rows (fixed-stride or condensed) in HBM, and sparse batches of
+//    them in host memory, where order gains little, claim rows in an open-addressing hash
+//    table instead: inside the fetch for host rows (hidden behind PCIe), in a claim pass
+//    that lists the distinct rows for HBM rows.  Repeats (Zipf mini-batches repeat hot
 //    rows a lot) copy their first occurrence's output row: inside the fetch for host rows,
 //    once that row is published in the table (so the copies overlap the PCIe reads), and
 //    in a copy kernel afterwards for the other modes.
@@ -256,7 +256,7 @@ fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
 template <typename U, int NC, bool EXACT, bool ASYNC>
 __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr bool kClaims = !EXACT && !ASYNC;  // in-fetch claims: fixed-stride host rows
+    constexpr bool kClaims = !ASYNC;  // in-fetch claims: host rows (fixed-stride or condensed)
     const int lane = threadIdx.x & 31;
     U *slots = reinterpret_cast<U *>(smem) +
                (int64_t)(threadIdx.x >> 5) * a.slots * (ASYNC ? 2 : 1) * a.slot_words;
@@ -570,11 +570,13 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         return IBP_ERR_UNSUPPORTED;
     }
     const int mode = fetch_dedup_mode();
-    if (mode == 2 || (mode == 0 && !offsets && impl != 2 && (on_device || 4 * nidx < n))) {
-        // fixed-stride compressed rows in HBM, or a sparse batch of them in host memory:
-        // claim rows in a hash table instead of sorting (HBM does not care about row order,
-        // and far-apart host rows gain little from it; condensed and raw rows and dense host
-        // batches do lose without it, so they keep the sort)
+    if (mode == 2 || (mode == 0 && impl != 2 && (on_device || 4 * nidx < n))) {
+        // compressed rows (fixed-stride or condensed) in HBM, or a sparse batch of them in
+        // host memory: claim rows in a hash table instead of sorting (HBM does not care about
+        // row order, and far-apart host rows gain little from it).  Dense host batches keep
+        // the sort: reading their rows in order pays when few of them repeat (uniform batches
+        // of a quarter to all of the set: 3-10% faster sorted), though skewed dense batches
+        // are faster hashed (mode 2); raw gathers gain nothing from claims.
         const int64_t slots = hash_slots(nidx);
         int64_t *hkeys = c.take<int64_t>(slots);
         int64_t *hpos = c.take<int64_t>(slots);

@@ -79,11 +79,12 @@ def test_dedup_modes_condensed(ibp, mode):
 @pytest.mark.parametrize("pattern", ["zipf", "one_row", "pairs"])
 @pytest.mark.parametrize("aligned", [True, False], ids=["out16", "out8"])
 @pytest.mark.parametrize("where", ["host", "device"])
-def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where):
+@pytest.mark.parametrize("layout", ["fixed", "condensed"])
+def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where, layout):
     """Hash claims (made inside the fetch for host rows, by a claim pass for device rows):
-    each repeat copies its first occurrence's output row inside the fetch, once that row is
-    published in the table.  Every row must be exact, into 16-byte aligned and unaligned
-    outputs, and no wait may give up (status bit 3)."""
+    each repeat copies its first occurrence's output row once that row is published in the
+    table.  Every row must be exact, for fixed-stride and condensed rows, into 16-byte aligned
+    and unaligned outputs, and no wait may give up (status bit 3)."""
     import ctypes
     from invariantbitpacking_b200 import _capi
     lib = _capi.lib
@@ -92,6 +93,9 @@ def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where):
     d = make(rng, n, v, 8)
     x = torch.from_numpy(d.copy()).pin_memory()
     m, b = ibp.preprocess(x, None)
+    if layout == "condensed":
+        ccomp, offs = ibp.compress_condensed(x, m, b)
+        offs = offs.cuda()
     bm = ibp.compress_inplace(x, m, b)
     cl = ibp.get_single_compress_len(x, m, b)
     torch.cuda.synchronize()
@@ -106,6 +110,8 @@ def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where):
     idx = idx.astype(np.int64)
     if where == "device":
         x = x.cuda()
+        if layout == "condensed":
+            ccomp = ccomp.cuda()
     ti = torch.from_numpy(idx).cuda()
     nidx = idx.size
     buf = torch.full((nidx * v + 1,), 7, dtype=torch.int64, device="cuda")
@@ -115,9 +121,14 @@ def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where):
     st = torch.cuda.current_stream().cuda_stream
     _capi.check(lib.ibp_set_fetch_dedup(2))
     try:
-        _capi.check(lib.ibp_decompress_fetch(x.data_ptr(), n, v, 8, m.data_ptr(), b.data_ptr(),
-                                             bm.data_ptr(), ti.data_ptr(), nidx, cl,
-                                             out.data_ptr(), -1, -1, -1, ws.data_ptr(), wsb, st))
+        if layout == "fixed":
+            _capi.check(lib.ibp_decompress_fetch(
+                x.data_ptr(), n, v, 8, m.data_ptr(), b.data_ptr(), bm.data_ptr(), ti.data_ptr(),
+                nidx, cl, out.data_ptr(), -1, -1, -1, ws.data_ptr(), wsb, st))
+        else:
+            _capi.check(lib.ibp_decompress_fetch_condensed(
+                ccomp.data_ptr(), ccomp.numel(), offs.data_ptr(), n, v, 8, m.data_ptr(),
+                b.data_ptr(), ti.data_ptr(), nidx, out.data_ptr(), ws.data_ptr(), wsb, st))
         status = ctypes.c_int32(-1)
         _capi.check(lib.ibp_read_status(ws.data_ptr(), ctypes.byref(status), st))
     finally:
