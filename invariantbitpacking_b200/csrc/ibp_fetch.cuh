@@ -191,6 +191,65 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
     }
 }
 
+// decode_row for up to kRowsInFlight rows of at most 64 words at once (rows in slots
+// `slots + q * slot_words` for the q set in `qm`, outputs `o[q]`): the prefix sums of every
+// row's chunks are issued together, so their shuffle chains overlap instead of following
+// one another, then each row's bits are placed as in decode_row.
+template <typename U, int NC>
+__device__ __forceinline__ void decode_rows_multi(const U *__restrict__ slots,
+                                                  int64_t slot_words, unsigned qm, int64_t v,
+                                                  int64_t mw, const LaneTables<U, NC> &lt,
+                                                  U *const *o) {
+    static_assert(NC > 0, "register tables only");
+    constexpr int W = 8 * sizeof(U);
+    constexpr int Q = kRowsInFlight;
+    const int lane = threadIdx.x & 31;
+    int incl[Q][NC];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const uint32_t *units = reinterpret_cast<const uint32_t *>(slots + q * slot_words);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int64_t j = 32 * c + lane;
+            const bool in = ((qm >> q) & 1) && j < v;
+            const bool cj = in && ((units[j >> 5] >> (j & 31)) & 1u);
+            incl[q][c] = in ? (cj ? lt.nb[c] : W) : 0;
+        }
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int y = __shfl_up_sync(0xffffffffu, incl[q][c], off);
+                if (lane >= off) incl[q][c] += y;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (!((qm >> q) & 1)) continue;
+        const U *buf = slots + q * slot_words;
+        const uint32_t *units = reinterpret_cast<const uint32_t *>(buf);
+        const U *stream = buf + mw;
+        int64_t base = 0;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (32 * c >= v) break;
+            const int64_t j = 32 * c + lane;
+            const bool in = j < v;
+            const bool cj = in && ((units[j >> 5] >> (j & 31)) & 1u);
+            const int L = in ? (cj ? lt.nb[c] : W) : 0;
+            if (in) {
+                const U y = get_bits<U>(stream, base + incl[q][c] - L, L);
+                o[q][j] = cj ? (U)(lt.bv[c] | scatter_regs<U>(y, (U)~lt.m[c], lt.mv[c])) : y;
+            }
+            base += __shfl_sync(0xffffffffu, incl[q][c], 31);
+        }
+    }
+}
+
 // Exact compressed words of the row whose bitmap is in the slot (bitmap + stream).
 template <typename U, int NC>
 __device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t v, int64_t mw,
@@ -220,7 +279,7 @@ __device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t 
 // bitmaps, the rest of every row that needs more than its first read (all issued before any
 // is waited for: 16-byte blocks in registers, at most 32 per row; longer tails and
 // unaligned rows take the plain loop), then the decode (or copy, for rows stored raw).
-template <typename U, int NC>
+template <typename U, int NC, bool MULTI = false>
 __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables<U, NC> &lt,
                                             U *__restrict__ slots, int64_t slot_words,
                                             const int *lid, int cnt, int64_t key, U *orow,
@@ -262,6 +321,36 @@ __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables
                 reinterpret_cast<uint4 *>(slots + q * slot_words)[tb0[q] + lane] = tail[q];
     }
     __syncwarp();
+    if constexpr (MULTI && NC > 0) {
+        // rows of at most 64 words: copies and corrupt rows first, then every row of the
+        // group that decodes from its slot, all at once
+        U *o[kRowsInFlight];
+        unsigned qm = 0;
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            o[q] = nullptr;
+            if (q < cnt) {
+                const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+                o[q] = reinterpret_cast<U *>(
+                    __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
+                if (end[q] < 0) {
+                    warp_copy<U>(o[q], s.comp + r * v, v);
+                } else if (end[q] >= v) {
+                    if (lane == 0) atomicOr(status, kStatusCorruptRow);
+                } else if (end[q] + 2 > slot_words) {  // not with slots of v + 2 words
+                    decode_row<U, NC>(s.comp + r * v, v, s.mw, s.t, lt, o[q]);
+                    __syncwarp();
+                } else {
+                    if (lane < 2) slots[q * slot_words + end[q] + lane] = 0;
+                    qm |= 1u << q;
+                }
+            }
+        }
+        __syncwarp();
+        if (qm) decode_rows_multi<U, NC>(slots, slot_words, qm, v, s.mw, lt, o);
+        __syncwarp();
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < kRowsInFlight; ++q) {
         if (q < cnt) {
@@ -430,8 +519,8 @@ __device__ __forceinline__ void fetch_heads_async(const RowSet<U> &s, const Lane
             cp_async_wait_all();
         }
         __syncwarp();
-        finish_rows<U, NC>(s, lt, slots + (int64_t)cur * nslots * slot_words, slot_words, lid,
-                           cnt, key, orow, packed, status);
+        finish_rows<U, NC, true>(s, lt, slots + (int64_t)cur * nslots * slot_words, slot_words,
+                                 lid, cnt, key, orow, packed, status);
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < kRowsInFlight; ++q) lid[q] = nlid[q];
