@@ -13,6 +13,12 @@ measured in the same run.  `--impl reference` times the CPU restatement of the r
 algorithm on the host cores (the reference implementation has no CPU path of its own).
 Under torchrun every rank runs an independent replica on its own GPU (the path has no
 exchange step); time is the max over ranks.
+
+Other lines (`--config`): embedding_tables and decoder_layer (batched multi-set fetch),
+served_mix (the server against per-request fetches), embedding_bag (cache-miss fetch shim),
+host_rows and device_rows (whole-set decompression against the reference's GPU build), and
+device_graph_features (the graph-feature batches from a device-resident copy of the set,
+against the HBM roofline).
 """
 import argparse
 import ctypes
@@ -45,7 +51,8 @@ def parse():
     ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--config", default="graph_features",
                     choices=["graph_features", "embedding_tables", "decoder_layer",
-                             "served_mix", "embedding_bag", "device_rows", "host_rows"])
+                             "served_mix", "embedding_bag", "device_rows", "host_rows",
+                             "device_graph_features"])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=300)
     ap.add_argument("--shard", action="store_true",
@@ -418,6 +425,118 @@ def reference_gpu(torch, comp, m, b, bm, comp_len, batches_dev, steps):
             "ms_per_step": round(ms / steps, 3), "steps": steps,
             "what": "reference decompress_fetch (its sources built for sm_100a, default impl, "
                     "nblks=2*SMs) on the same compressed rows and index arrays"}, out
+
+
+def run_device_graph(args):
+    """The graph-feature fetch from a device-resident copy of the compressed set (the
+    `--rows` rows compressed in place on the host, then copied to HBM): the same Zipf(1.1)
+    mini-batches, index on the device, one decompress_fetch per step.  Reports delivered
+    GB/s, the call against the HBM roofline (compressed bytes of the distinct rows read +
+    every output row written, over the measured HBM copy bandwidth), the row-fetch kernel
+    alone, and the reference's decompress_fetch on the same device rows."""
+    import torch
+    import invariantbitpacking_b200 as ibp
+    from invariantbitpacking_b200 import _capi
+    lib = _capi.lib
+    d, batches = make_workload(args.rows)
+    x = torch.from_numpy(d).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    comp_len = ibp.get_single_compress_len(x, m, b)
+    sizes = ibp.get_compress_size(x, m, b)
+    bm = ibp.compress_inplace(x, m, b)
+    torch.cuda.synchronize()
+    sizes_np = sizes.cpu().numpy()
+    xd = x.cuda()
+    bdev = [torch.from_numpy(bt).cuda() for bt in batches]
+    uniq = [np.unique(bt) for bt in batches]
+    nmax = max(len(bt) for bt in batches)
+    out = torch.empty((nmax, V), dtype=torch.int64, device="cuda")
+    wsb = lib.ibp_decompress_fetch_workspace_size(nmax, V, 8, 1)
+    wsp = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(k):
+        idx = bdev[k % len(bdev)]
+        _capi.check(lib.ibp_decompress_fetch(
+            xd.data_ptr(), args.rows, V, 8, m.data_ptr(), b.data_ptr(), bm.data_ptr(),
+            idx.data_ptr(), idx.shape[0], comp_len, out.data_ptr(), -1, -1, -1, wsp.data_ptr(),
+            wsb, stream.cuda_stream))
+        return k % len(bdev)
+
+    for k in range(len(batches)):
+        step(k)
+        torch.cuda.synchronize()
+        assert np.array_equal(out[:len(batches[k])].cpu().numpy(), d[batches[k]]), \
+            "device-resident fetch mismatch"
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        hbm_peak, hbm_src = float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except Exception:
+        hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
+    n0 = lib.ibp_kernel_launch_count()
+    _capi.check(lib.ibp_profile_enable(args.steps))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    rows = call_bytes = kern_bytes = 0
+    with Clocks(torch.cuda.current_device()) as clk:
+        e0.record()
+        for k in range(args.steps):
+            j = step(k)
+            rows += len(batches[j])
+            comp_b = int(sizes_np[uniq[j]].sum())
+            call_bytes += comp_b + len(batches[j]) * V * 8
+            kern_bytes += comp_b + len(uniq[j]) * V * 8
+        e1.record()
+        e1.synchronize()
+    launches = lib.ibp_kernel_launch_count() - n0
+    ms = e0.elapsed_time(e1)
+    buf = (ctypes.c_float * args.steps)()
+    got = lib.ibp_profile_take(buf, args.steps)
+    kms = sum(buf[i] for i in range(got))
+    kern_share = got / args.steps
+    call_gbs = call_bytes / ms / 1e6
+    kern_gbs = kern_bytes * kern_share / kms / 1e6
+    ref = None
+    if not args.no_reference_gpu:
+        try:
+            r = reference_gpu(torch, xd, m, b, bm, comp_len, bdev, args.steps)
+            if r is not None:
+                ref, rout = r
+                torch.cuda.synchronize()
+                ref["bit_exact_vs_input"] = bool(
+                    np.array_equal(rout.cpu().numpy(), d[batches[0]]))
+        except Exception as exc:  # reported, not fatal
+            ref = {"error": repr(exc)[:200]}
+    line = {
+        "metric": "decompress_fetch delivered GB/s (graph features, Zipf 1.1 mini-batches, "
+                  "device-resident)",
+        "value": round(rows * V * 8 / ms / 1e6, 3), "unit": "GB/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic",
+        "config": {"workload": f"device_graph_features: {args.rows} graph-feature rows of 64 "
+                               "int64 words compressed in place, copied to HBM",
+                   "rows": args.rows, "vec_words": V, "batches": BATCH_DESC,
+                   "comp_len_words": comp_len,
+                   "l2": "outputs of 51-205 MB per step; the compressed set is "
+                         f"{x.numel() * 8 / 1e9:.2f} GB"},
+        "roofline": {"bound": "hbm", "achieved": round(call_gbs, 1), "peak": hbm_peak,
+                     "unit": "GB/s", "frac": round(call_gbs / hbm_peak, 4), "traffic": None,
+                     "what": "whole call: compressed bytes of the distinct rows read + every "
+                             "output row written, over the call's CUDA-event time",
+                     "peak_source": hbm_src},
+        "fetch_kernel": {"achieved": round(kern_gbs, 1), "frac": round(kern_gbs / hbm_peak, 4),
+                         "unit": "GB/s",
+                         "ms_per_launch": round(kms / max(got, 1), 4),
+                         "what": "row-fetch kernel alone: compressed bytes read + decoded "
+                                 "bytes written of the distinct rows / its CUDA-event time"},
+        "reference_gpu": ref,
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
 
 
 def kmeans_vs_reference(torch, ibp, arrays):
@@ -1023,6 +1142,13 @@ def main():
                               "time the reference's GPU build in the same line"}))
             return
         run_rows(args, args.config.split("_")[0])
+        return
+    if args.config == "device_graph_features":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the device-resident "
+                              "configuration times the reference's GPU build in the same line"}))
+            return
+        run_device_graph(args)
         return
     if args.config == "embedding_bag":
         if args.impl == "reference":
