@@ -1196,6 +1196,7 @@ def main():
     batches_dev = [torch.from_numpy(bt).cuda() for bt in batches]
     batches_host = [torch.from_numpy(bt).pin_memory() for bt in batches]
     uniq_bytes = [int(sizes_np[np.unique(bt)].sum()) for bt in batches]
+    uniq_rows = [len(np.unique(bt)) for bt in batches]
     all_bytes = [int(sizes_np[bt].sum()) for bt in batches]
     maxb = max(len(bt) for bt in batches)
     out = torch.empty((maxb, V), dtype=torch.int64, device="cuda")
@@ -1249,6 +1250,10 @@ def main():
     kall = [all_bytes[k % len(batches)] for k in range(args.steps)]
     fetch_gbs = sum(kuniq) / sum(kms) / 1e6
     fetch_gbs_dups = sum(kall) / sum(kms) / 1e6
+    # host-memory bytes the kernel reads per launch: the ncu capture of this kernel on the
+    # 400k-row batch read 714,969 sysmem sectors for its 79,441 distinct rows (9.0 sectors,
+    # 288 bytes, per row: the 264-byte rows are read as whole 32-byte sectors)
+    traffic = 288.0 * sum(uniq_rows[k % len(batches)] for k in range(args.steps)) / args.steps
 
     # ---- e2e: public API, index uploaded per step, last row read back per step
     res_host = torch.empty(V, dtype=torch.int64).pin_memory()
@@ -1433,7 +1438,12 @@ def main():
                             "pinned host (on a copy stream, one step ahead) and the last output "
                             "row read back"},
             "roofline": {"bound": "pcie", "achieved": round(fetch_gbs, 3), "peak": round(pcie, 3),
-                         "unit": "GB/s", "frac": round(fetch_gbs / pcie, 4), "traffic": None,
+                         "unit": "GB/s", "frac": round(fetch_gbs / pcie, 4),
+                         "traffic": int(traffic),
+                         "traffic_what": "host-memory (PCIe) bytes read per launch: 288 B per "
+                                         "distinct row (ncu sysmem read sectors of the 400k-row "
+                                         "batch, 9.0 per row) x distinct rows; algorithmic: "
+                                         f"{int(sum(kuniq) / len(kuniq))} B per launch",
                          "what": "fetch_rows_kernel: compressed bytes of the distinct rows of "
                                  "each batch / kernel CUDA-event time",
                          "peak_source": "pinned host->device copy measured in this run "
