@@ -173,7 +173,6 @@ def test_batch_sorted_after_capture_and_bad_rows(ibp, sets):
 
 
 def test_batch_sorted_total_mismatch_is_flagged(ibp, sets):
-    import ctypes
     from invariantbitpacking_b200 import _capi
     from invariantbitpacking_b200.batch import SetRegistry
     reg = SetRegistry([s[1] for s in sets[:1]])

@@ -7,8 +7,6 @@ arrays, word sizes and row lengths, so whatever the first call leaves in the sha
 must not leak into the second -- and against the source rows.  A call that needs more
 scratch than the static array holds is refused before anything runs.  This file is named so
 that pytest collects it last."""
-import ctypes
-
 import numpy as np
 import pytest
 import torch
