@@ -543,6 +543,55 @@ def run_device_graph(args):
     print(json.dumps(line), flush=True)
 
 
+def reference_per_call(torch, sets, variants, outs, step_bytes, arrays, warmup, steps):
+    """The reference's decompress_fetch (its sources built for sm_100a, oracle/_ref) called
+    the way its callers do: one call per tensor set per step, on the same compressed sets,
+    index arrays and output tensors; None when the reference is not built.  Every output of
+    the first pass over the request variants is checked against the source rows."""
+    import glob
+    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    if not mods:
+        return None
+    sys.path.insert(0, os.path.dirname(mods[0]))
+    import ibp_cuda as ref
+    ref.print_debug(False)
+    # the reference compares the output tensor's device with this one, index included
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def step(j):
+        for (sid, idx, first, count), oo in zip(variants[j], outs[j]):
+            x, m, b, bm, cl = sets[sid]
+            ref.decompress_fetch(x, m, b, bm, dev, cl, idx, None, None, None, oo)
+
+    exact = True
+    for j in range(len(variants)):
+        for oo in outs[j]:
+            oo.zero_()
+        step(j)
+        torch.cuda.synchronize()
+        for (sid, idx, first, count), oo in zip(variants[j], outs[j]):
+            want = (arrays[sid][idx.cpu().numpy()] if idx is not None
+                    else arrays[sid][first:first + count])
+            exact = exact and bool(np.array_equal(oo.cpu().numpy(), want))
+    for k in range(warmup):
+        step(k % len(variants))
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tot = 0
+    a.record()
+    for k in range(steps):
+        j = k % len(variants)
+        step(j)
+        tot += step_bytes[j]
+    e.record()
+    e.synchronize()
+    ms = a.elapsed_time(e)
+    return {"value": round(tot / ms / 1e6, 3), "unit": "GB/s", "ms_per_step": round(ms / steps, 4),
+            "steps": steps, "bit_exact_vs_input": exact,
+            "what": f"reference decompress_fetch, one call per set per step (its sources built "
+                    f"for sm_100a, default impl, nblks=2*SMs), same sets, indices and outputs"}
+
+
 def kmeans_vs_reference(torch, ibp, arrays):
     """preprocess_kmeans (16 clusters) on the three smallest tables viewed as int32 rows of 64
     words, ours against the reference's (built from its sources for sm_100a; its 8-byte
@@ -709,6 +758,12 @@ def run_batched(args):
     s1.record()
     s1.synchronize()
     sms = s0.elapsed_time(s1)
+    ref_steps = min(args.steps, 100)
+    try:
+        ref_call = reference_per_call(torch, sets, variants, outs, step_bytes, arrays,
+                                      args.warmup, ref_steps)
+    except Exception as exc:  # reported, not fatal
+        ref_call = {"error": repr(exc)[:200]}
     pcie = measured_pcie_h2d(torch)
     kavg = sum(kms) / max(len(kms), 1)
     ach = (sum(comp_bytes[k % len(variants)] for k in range(nk)) / sum(kms) / 1e6) if kms else None
@@ -732,6 +787,7 @@ def run_batched(args):
         "per_call": {"value": round(ptot / pms / 1e6, 3), "unit": "GB/s",
                      "ms_per_step": round(pms / args.steps, 4),
                      "what": f"{nsets} ibp.decompress_fetch calls per step, one per set"},
+        "reference_per_call": ref_call,
         "sorted_batch": {"value": round(stot / sms / 1e6, 3), "unit": "GB/s",
                          "ms_per_step": round(sms / args.steps, 4),
                          "what": "one ibp_batch_fetch_sorted per step (device sort, repeats "
