@@ -17,6 +17,9 @@ Behavioural differences from the reference, all deliberate:
     a temporary copy when it is not int64);
   * decompress_fetch rejects impl 3/4 (the reference's upper-bound stand-ins that do not
     decompress) and ignores nblks/nthreads values that do not fit the engine's kernels;
+  * decompress_fetch reads an out_device of "cuda" without an index as the current device,
+    so an output_tensor there passes the device check (the reference compares the
+    unindexed device with the tensor's and refuses);
   * preprocess_kmeans breaks distance ties toward the highest centroid id (the reference
     races) and accepts keyword-only `seed_rows` to fix the centroid seeds.
 """
