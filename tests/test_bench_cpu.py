@@ -41,3 +41,29 @@ def test_cpu_core_sweep_small():
     assert [e["cores"] for e in r["gather_copy"]] == cores
     assert all(e["value"] > 0 for e in r["decompress"] + r["gather_copy"])
     assert r["compress"]["value"] > 0
+
+
+def test_clock_summary_keeps_samples_inside_the_region():
+    """bench.Clocks.summary on fake nvidia-smi lines: only samples taken inside the timed
+    region count, throttle reasons are collected from them, and a region shorter than one
+    sampling period keeps the sample nearest its middle."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.Clocks(0)
+    c.t0, c.t1 = 10.0, 10.1
+    c.lines = [
+        (9.90, "1000, 1965, 500, Not Active, Not Active, Not Active, Active"),  # before
+        (10.02, "1965, 1965, 900, Not Active, Not Active, Not Active, Not Active"),
+        (10.06, "1900, 1965, 950, Not Active, Not Active, Not Active, Active"),
+        (10.09, "1950, 1965, 940, Not Active, Not Active, Not Active, Not Active"),
+        (10.30, "700, 1965, 300, Active, Not Active, Not Active, Not Active"),  # after
+        (10.31, "garbage line"),
+    ]
+    s = c.summary()
+    assert s["samples"] == 3 and s["sm_mhz"] == 1950.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"]
+    c.t0, c.t1 = 10.03, 10.035
+    s = c.summary()
+    assert s["samples"] == 1 and s["sm_mhz"] == 1965.0
+    c.lines = []
+    assert bench.Clocks(0).summary()["samples"] == 0
