@@ -20,7 +20,7 @@ ibp_cuda.print_debug(False)
 __all__ = ["print_debug", "preprocess", "preprocess_kmeans", "get_compress_size",
            "get_single_compress_len", "compress_inplace", "compress", "compress_condensed",
            "decompress_fetch_condensed",
-           "decompress_fetch", "read_shared", "ibp_cuda", "IBPError"]
+           "decompress_fetch", "read_shared", "set_fetch_dedup", "ibp_cuda", "IBPError"]
 
 
 def print_debug(flag):
@@ -82,3 +82,20 @@ def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, device, in
 
 def read_shared(filename, shape, dtype):
     return ibp_cuda.read_shared(filename, shape, dtype)
+
+
+_DEDUP_MODES = {"auto": 0, "sort": 1, "hash": 2}
+
+
+def set_fetch_dedup(mode):
+    """How decompress_fetch finds the repeated rows of an index array, process-wide (no
+    counterpart in the reference, which always sorts): "auto" (hash table for compressed rows
+    in device memory and for sparse host batches, else sort), "sort", or "hash" (repeats are
+    then copied inside the fetch for host rows).  Dense batches whose rows repeat a lot are
+    faster with "hash", dense batches with few repeats with "sort".  Also takes 0/1/2."""
+    from . import _capi
+    m = _DEDUP_MODES.get(mode, mode) if isinstance(mode, str) else mode
+    if m not in (0, 1, 2):
+        raise ValueError(f"set_fetch_dedup: mode must be one of {sorted(_DEDUP_MODES)} "
+                         f"or 0/1/2, got {mode!r}")
+    _capi.check(_capi.lib.ibp_set_fetch_dedup(int(m)))

@@ -119,3 +119,20 @@ def test_read_shared_round_trip(tmp_path):
     a.tofile(f)
     t = ibp.read_shared(str(f), [3, 5], torch.float32)
     assert t.is_shared() and np.array_equal(t.numpy(), a)
+
+
+def test_set_fetch_dedup_modes():
+    """The dedup knob is a host-side setting: names and numbers are accepted, anything else
+    is refused by the Python layer and by the C ABI, and auto is restored."""
+    import invariantbitpacking_b200 as ibp
+    from invariantbitpacking_b200 import _capi
+    try:
+        for m in ("sort", "hash", "auto", 1, 2, 0):
+            ibp.set_fetch_dedup(m)
+        for bad in ("fast", 3, -1):
+            with pytest.raises(ValueError):
+                ibp.set_fetch_dedup(bad)
+        with pytest.raises(_capi.IBPError):
+            _capi.check(_capi.lib.ibp_set_fetch_dedup(7))
+    finally:
+        ibp.set_fetch_dedup("auto")
