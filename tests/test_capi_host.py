@@ -88,28 +88,84 @@ def test_dropin_rejects_unpinned_host_tensors_with_reference_messages():
         ibp.decompress_fetch(x, m, m, torch.zeros(1, dtype=torch.int32), "cuda")
 
 
-def test_dropin_signatures_match_reference():
-    """Positional signatures of the reference's `ibp` package (ibp/__init__.py:8-41)."""
+# Positional parameters of every export of the reference's extension module ibp_cuda
+# (src/ibp_api.cu:20-40 declarations, :124-135 bindings; pybind11 gives none a default).
+REF_EXTENSION_ARITY = {"print_debug": 1, "preprocess": 2, "preprocess_kmeans": 3,
+                       "get_compress_size": 5, "compress_inplace": 4, "compress_condensed": 4,
+                       "decompress_fetch": 11, "read_shared": 3}
+# Positional parameters of the reference's `ibp` package (ibp/__init__.py:8-41).
+REF_PACKAGE_PARAMS = {
+    "preprocess": ["dataset", "threshold"],
+    "preprocess_kmeans": ["dataset", "centroids", "threshold"],
+    "get_compress_size": ["dataset", "mask", "bitval", "index_arr", "compress_total"],
+    "get_single_compress_len": ["dataset", "mask", "bitval", "index_arr"],
+    "compress_inplace": ["dataset", "mask", "bitval", "index_arr"],
+    "compress": ["dataset", "mask", "bitval", "index_arr"],
+    "decompress_fetch": ["comp_dataset", "mask", "bitval", "bitmask", "device", "comp_len",
+                         "index_arr", "nblks", "nthds", "imp", "output_tensor"],
+}
+
+
+def _positional(fn):
     import inspect
+    sig = inspect.signature(fn)
+    return sig, [p for p in sig.parameters.values()
+                 if p.kind in (p.POSITIONAL_ONLY, p.POSITIONAL_OR_KEYWORD)]
+
+
+def _check_extension_arity(mod):
+    for fn, n in REF_EXTENSION_ARITY.items():
+        sig, pos = _positional(getattr(mod, fn))
+        assert len(pos) == n, (fn, len(pos))
+        sig.bind(*range(n))  # the reference's full positional call binds
+
+
+def test_dropin_signatures_match_reference():
+    """The package mirrors ibp/__init__.py's positional signatures, and its ibp_cuda mirrors
+    the extension's: every export takes exactly the reference's positional arguments."""
     import invariantbitpacking_b200 as ibp
-    want = {
-        "preprocess": ["dataset", "threshold"],
-        "preprocess_kmeans": ["dataset", "centroids", "threshold"],
-        "get_compress_size": ["dataset", "mask", "bitval", "index_arr", "compress_total"],
-        "get_single_compress_len": ["dataset", "mask", "bitval", "index_arr"],
-        "compress_inplace": ["dataset", "mask", "bitval", "index_arr"],
-        "compress": ["dataset", "mask", "bitval", "index_arr"],
-        "decompress_fetch": ["comp_dataset", "mask", "bitval", "bitmask", "device", "comp_len",
-                             "index_arr", "nblks", "nthds", "imp", "output_tensor"],
-    }
-    for fn, params in want.items():
-        sig = inspect.signature(getattr(ibp, fn))
-        pos = [p.name for p in sig.parameters.values()
-               if p.kind in (p.POSITIONAL_ONLY, p.POSITIONAL_OR_KEYWORD)]
-        assert pos == params, fn
-    for fn in ("print_debug", "preprocess", "preprocess_kmeans", "get_compress_size",
-               "compress_inplace", "compress_condensed", "decompress_fetch", "read_shared"):
-        assert callable(getattr(ibp.ibp_cuda, fn))
+    for fn, params in REF_PACKAGE_PARAMS.items():
+        _, pos = _positional(getattr(ibp, fn))
+        assert [p.name for p in pos] == params, fn
+    _check_extension_arity(ibp.ibp_cuda)
+
+
+def test_dropin_directory_imports_as_ibp_and_ibp_cuda():
+    """With dropin/ on sys.path, `import ibp` and `import ibp_cuda` (the reference's import
+    lines) resolve to the engine, with the reference's signatures; checked in a fresh
+    interpreter whose sys.path holds dropin/ but not the repository root."""
+    import json
+    import subprocess
+    import sys
+    code = r"""
+import json, sys, inspect
+import torch
+import ibp
+import ibp_cuda
+import invariantbitpacking_b200.ibp_cuda as mirror
+out = {"ibp_file": ibp.__file__, "ibp_cuda_file": ibp_cuda.__file__,
+       "same": ibp_cuda.decompress_fetch is mirror.decompress_fetch,
+       "pkg": {fn: [p.name for p in inspect.signature(getattr(ibp, fn)).parameters.values()]
+               for fn in ("preprocess", "preprocess_kmeans", "get_compress_size",
+                          "get_single_compress_len", "compress_inplace", "compress",
+                          "decompress_fetch")},
+       "ext": {fn: len([p for p in inspect.signature(getattr(ibp_cuda, fn)).parameters.values()
+                        if p.kind in (p.POSITIONAL_ONLY, p.POSITIONAL_OR_KEYWORD)])
+               for fn in ("print_debug", "preprocess", "preprocess_kmeans", "get_compress_size",
+                          "compress_inplace", "compress_condensed", "decompress_fetch",
+                          "read_shared")}}
+print(json.dumps(out))
+"""
+    env = dict(os.environ, PYTHONPATH=os.path.join(REPO, "dropin"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                       cwd="/", timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    assert got["ibp_file"] == os.path.join(REPO, "dropin", "ibp", "__init__.py")
+    assert got["ibp_cuda_file"] == os.path.join(REPO, "dropin", "ibp_cuda.py")
+    assert got["same"]
+    assert got["pkg"] == REF_PACKAGE_PARAMS
+    assert got["ext"] == REF_EXTENSION_ARITY
 
 
 def test_read_shared_round_trip(tmp_path):
@@ -136,3 +192,12 @@ def test_set_fetch_dedup_modes():
             _capi.check(_capi.lib.ibp_set_fetch_dedup(7))
     finally:
         ibp.set_fetch_dedup("auto")
+
+
+def test_noalloc_limit_constant_matches_header():
+    from invariantbitpacking_b200 import _capi
+    m = re.search(r"#define\s+IBP_NOALLOC_SCRATCH_BYTES\s+(\d+)", open(HEADER).read())
+    assert m and int(m.group(1)) == _capi.NOALLOC_SCRATCH_BYTES == 4 << 20
+    # the documented fit test: the workspace query of the regular entry point
+    assert _capi.lib.ibp_decompress_fetch_workspace_size(80_000, 64, 8, 1) <= 4 << 20
+    assert _capi.lib.ibp_decompress_fetch_workspace_size(120_000, 64, 8, 1) > 4 << 20
