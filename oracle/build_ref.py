@@ -11,7 +11,8 @@ a GPU box, where tests/golden/make_golden.py runs it to dump golden vectors).
 
 Nothing in the product imports this module or its output.
 
-Usage: python oracle/build_ref.py [--ref /root/reference] [--jobs 4]
+Usage: python oracle/build_ref.py --ref <reference checkout> [--jobs 4]
+       (or set IBP_REFERENCE_DIR to the checkout and omit --ref)
 """
 import argparse
 import concurrent.futures as cf
@@ -38,7 +39,16 @@ def _flags():
     return incs, abi
 
 
-def build(ref="/root/reference", jobs=4, quiet=False):
+def reference_dir():
+    """The reference checkout named by IBP_REFERENCE_DIR, or None."""
+    ref = os.environ.get("IBP_REFERENCE_DIR")
+    return ref if ref and os.path.isdir(os.path.join(ref, "src")) else None
+
+
+def build(ref=None, jobs=4, quiet=False):
+    ref = ref or reference_dir()
+    if not ref:
+        raise FileNotFoundError("no reference checkout: pass --ref or set IBP_REFERENCE_DIR")
     if not os.path.isdir(os.path.join(ref, "src")):
         raise FileNotFoundError(f"reference sources not found under {ref}")
     os.makedirs(os.path.join(OUT, "obj"), exist_ok=True)
@@ -82,7 +92,8 @@ def build(ref="/root/reference", jobs=4, quiet=False):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None,
+                    help="reference checkout (default: $IBP_REFERENCE_DIR)")
     ap.add_argument("--jobs", type=int, default=4)
     a = ap.parse_args()
     build(a.ref, a.jobs)

@@ -19,18 +19,31 @@ Usage (on a machine with a B200 and the reference built into oracle/_ref):
 """
 import argparse
 import ctypes
+import glob
+import importlib.util
 import json
 import os
-import sys
 
 import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-sys.path.insert(0, os.path.join(REPO, "oracle", "_ref"))
-import ibp_cuda  # noqa: E402  (the reference extension)
 
+
+def _reference_extension():
+    """The reference extension, loaded by explicit file path from oracle/_ref (never whatever
+    module named ibp_cuda happens to be importable)."""
+    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    if not mods:
+        raise SystemExit("oracle/_ref/ibp_cuda*.so is missing: run oracle/build_ref.py first")
+    spec = importlib.util.spec_from_file_location("ibp_cuda", mods[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+ibp_cuda = _reference_extension()
 ibp_cuda.print_debug(False)
 LIBC = ctypes.CDLL("libc.so.6")
 

@@ -9,16 +9,38 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_reference_arm_prints_contract_line():
-    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--rows", "60000", "--steps", "2", "--warmup", "1"],
-                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    """The reference arm runs the GPU arm's exact configuration (whole-set mask sweep, whole
+    mini-batches) and loads nothing of the engine: the process never maps libibp_b200.so."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--rows', '60000', "
+            "'--steps', '2', '--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('ENGINE_MAPPED' if 'libibp_b200' in maps else 'ENGINE_NOT_MAPPED')")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                         timeout=600, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
-    line = json.loads(out.stdout.strip().splitlines()[-1])
+    lines = out.stdout.strip().splitlines()
+    assert lines[-1] == "ENGINE_NOT_MAPPED"
+    line = json.loads(lines[-2])
     for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
                 "higher_is_better", "config", "cpu_baseline", "e2e"):
         assert key in line, key
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+    # the same config dict the GPU arm builds for this run (mask and sizes from the oracle,
+    # which is bit-exact with the engine)
+    sys.path.insert(0, ROOT)
+    import bench
+    import oracle
+    d, _ = bench.make_workload(60000)
+    m, b, _ = oracle.preprocess(d, None)
+    sizes = oracle.compress_size(d, m, b)
+
+    class A:
+        rows = 60000
+    want = bench.headline_config(A, 1, False, 2, int(int(sizes.sum()) / d.nbytes * bench.V),
+                                 float(sizes.sum()) / d.nbytes)
+    assert line["config"] == json.loads(json.dumps(want))
+    assert "sample_rows_per_step" not in line["config"]
 
 
 def test_cpu_core_sweep_small():
