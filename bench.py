@@ -10,9 +10,17 @@ the index uploaded from pinned host memory and the last output row read back eac
 `roofline` is for the row-fetch kernel: compressed bytes of the distinct rows it reads over
 PCIe per launch / its CUDA-event duration, against the PCIe host-to-device copy bandwidth
 measured in the same run.  `--impl reference` times the CPU restatement of the reference
-algorithm on the host cores (the reference implementation has no CPU path of its own).
-Under torchrun every rank runs an independent replica on its own GPU (the path has no
-exchange step); time is the max over ranks.
+algorithm on the host cores, on exactly this configuration (whole-set mask sweep, whole
+mini-batches) and without loading the engine (the reference implementation has no CPU path
+of its own).  Under torchrun every rank runs an independent replica on its own GPU (the path
+has no exchange step); time is the max over ranks.
+
+The default line also carries the other named configurations, each measured in the same
+run: `plain_small` (16384 x 128 int64, 2048-row fetches: microseconds per call),
+`served_mix` (the continuous-batching server against per-request fetches, ours and the
+reference's, p50/p99 and GB/s at two arrival rates), `embedding_tables` and `decoder_layer`
+(batched multi-set fetches), and `value_1000_steps` (the headline over a long region).
+`--no-extras` leaves them out.
 
 Other lines (`--config`): embedding_tables and decoder_layer (batched multi-set fetch),
 served_mix (the server against per-request fetches), embedding_bag (cache-miss fetch shim),
@@ -40,6 +48,29 @@ BATCHES = (100_000, 200_000, 400_000)
 METRIC = "decompress_fetch delivered GB/s (graph features, Zipf 1.1 mini-batches, host-resident)"
 
 
+_REF_MODULE = None
+
+
+def reference_module():
+    """The reference's own extension module (its sources built for sm_100a into
+    oracle/_ref/ibp_cuda*.so), loaded by explicit file path so that no other module named
+    ibp_cuda on sys.path (a drop-in shim, say) can stand in for it; None when not built."""
+    global _REF_MODULE
+    if _REF_MODULE is None:
+        import glob
+        import importlib.util
+        mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+        if not mods:
+            return None
+        spec = importlib.util.spec_from_file_location("ibp_cuda", mods[0])
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        assert os.path.samefile(mod.__file__, mods[0])
+        mod.print_debug(False)
+        _REF_MODULE = mod
+    return _REF_MODULE
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -60,6 +91,10 @@ def parse():
                          "(strong scaling) instead of one replica per rank")
     ap.add_argument("--inflight", type=int, default=4,
                     help="served_mix: batches the server keeps on the GPU")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="graph_features: skip the other configurations' summaries")
+    ap.add_argument("--server-dedup", choices=["hash", "sort"], default="hash",
+                    help="served_mix: how the server's batches find repeated rows")
     ap.add_argument("--batch-mb", type=int, default=128,
                     help="served_mix: output MiB one server batch admits")
     return ap.parse_args()
@@ -170,8 +205,19 @@ class Clocks:
                 "samples": len(sm), "region_ms": round((t1 - self.t0) * 1e3, 1)}
 
 
+def synthetic_module():
+    """invariantbitpacking_b200/synthetic.py (numpy only), loaded by file path: importing it
+    through the package would load the engine's library, which the reference arm must not."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_ibp_synthetic", os.path.join(REPO, "invariantbitpacking_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def make_workload(rows, seed_batches=12):
-    from invariantbitpacking_b200 import synthetic
+    synthetic = synthetic_module()
     d = synthetic.graph_features(n=rows)
     z = synthetic.Zipf(rows, 1.1, seed=12)
     batches = [z.sample(BATCHES[i % len(BATCHES)]) for i in range(seed_batches)]
@@ -305,23 +351,42 @@ WORKLOAD = ("graph_features: 2.4M x 128 fp32 N(0,0.3^2), 8 mantissa bits, 30% ze
 BATCH_DESC = "Zipf(1.1) mini-batches cycling 100k/200k/400k rows"
 
 
+def headline_config(args, ws, shard, steps, comp_len, compressed_fraction):
+    """The `config` of the graph-feature line, shared by both arms so that they describe the
+    same workload: the batches a K-step run cycles through, the set and its compression."""
+    nrows_avg = sum(BATCHES[k % len(BATCHES)] for k in range(steps)) / steps
+    return {"workload": WORKLOAD, "rows": args.rows, "vec_words": V, "batches": BATCH_DESC,
+            "avg_rows_per_step": nrows_avg, "comp_len_words": int(comp_len),
+            "compressed_fraction": round(float(compressed_fraction), 4),
+            "mask": "preprocess threshold sweep (0.7..1.0) over the whole set",
+            "l2": "inputs larger than L2 (1.2 GB host set; 51-205 MB outputs)",
+            "parallelism": (f"each batch split into {ws} contiguous shards" if shard
+                            else f"{ws} independent replica(s)")}
+
+
 def run_reference_arm(args, ws, rank):
-    """CPU restatement of the reference algorithm on the host cores, same config/metric."""
+    """The reference algorithm on the host cores, on exactly the GPU arm's configuration: the
+    mask from the threshold sweep over the whole set, the whole set compressed in place, and
+    every step one whole mini-batch decompressed.  The reference implements decompress_fetch
+    only as a CUDA kernel (src/decompress.cu:10-156), so its CPU implementation is the oracle's
+    C restatement, run on all host threads.  Nothing of the engine is imported or loaded."""
     if rank != 0:
         return
     import oracle
-    from invariantbitpacking_b200 import synthetic  # noqa: F401
     d, batches = make_workload(args.rows)
-    m, b, _ = oracle.preprocess(d[:200_000], None)
-    comp, bm = oracle.compress(d, m, b)
     oracle.set_threads(os.cpu_count() or 1)
+    m, b, _ = oracle.preprocess(d, None)
+    sizes = oracle.compress_size(d, m, b)
+    comp_len = int(int(sizes.sum()) / d.nbytes * V)  # get_single_compress_len (ibp/__init__.py:22-29)
+    comp, bm = oracle.compress(d, m, b)
+    for k in range(len(batches)):  # the configuration is checked before it is timed
+        assert np.array_equal(oracle.decompress(comp, m, b, bm, batches[k]), d[batches[k]])
     for k in range(args.warmup):
-        oracle.decompress(comp, m, b, bm, batches[k % len(batches)][:20_000])
+        oracle.decompress(comp, m, b, bm, batches[k % len(batches)])
     t0 = time.perf_counter()
     rows = 0
-    per_step = max(1, int(60_000))
     for k in range(args.steps):
-        idx = batches[k % len(batches)][:per_step]
+        idx = batches[k % len(batches)]
         oracle.decompress(comp, m, b, bm, idx)
         rows += len(idx)
     el = time.perf_counter() - t0
@@ -331,18 +396,166 @@ def run_reference_arm(args, ws, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(el * 1e3 / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "vec_words": V, "batches": BATCH_DESC,
-                   "rows": args.rows, "sample_rows_per_step": per_step,
-                   "mask": "preprocess sweep on the first 200k rows"},
+        "config": headline_config(args, ws, args.shard and ws > 1, args.steps, comp_len,
+                                  float(sizes.sum()) / d.nbytes),
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s",
                          "cores": oracle.get_threads(), "kind": "port",
-                         "sample": f"{args.steps} steps of {per_step} rows of each mini-batch "
-                                   "decompressed on the host by the oracle (the reference "
-                                   "implements decompress_fetch only as a CUDA kernel)"},
+                         "sample": f"{args.steps} steps, each one whole mini-batch "
+                                   f"({rows} rows in all) decompressed on the host by the "
+                                   "oracle's C restatement of the reference's decompress_fetch "
+                                   "(which exists only as a CUDA kernel); on rank 0 only"},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def plain_small_summary(torch, ibp, lib, capi, pcie, steps, warmup):
+    """The small plain configuration: 16384 x 256 fp32 N(0, 0.5^2) with 5% of rows redrawn
+    from N(0, 100^2), viewed as int64 [16384 x 128], host-resident; preprocess at threshold
+    0.9, compress_inplace, then one decompress_fetch of 2048 distinct rows per call.  A latency
+    case: microseconds per call through the C ABI (index on the device) and through the
+    public API (index uploaded from pinned host memory, the last row read back, synchronised
+    every call), the fetch kernel's PCIe fraction, the reference's own decompress_fetch per
+    call on the same rows, and the setup's outputs against the oracle."""
+    import oracle
+    d, idx = synthetic_module().plain_small()
+    n, v = d.shape
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, 0.9)
+    bm = ibp.compress_inplace(x, m, b)
+    torch.cuda.synchronize()
+    om, ob, _ = oracle.preprocess(d, 0.9)
+    ocomp, obm = oracle.compress(d, om, ob)
+    sizes = oracle.compress_size(d, om, ob)
+    setup_exact = bool(np.array_equal(m.cpu().numpy(), om.view(np.int64))
+                       and np.array_equal(b.cpu().numpy(), ob.view(np.int64))
+                       and np.array_equal(bm.cpu().numpy(), obm)
+                       and np.array_equal(x.numpy(), ocomp.view(np.int64)))
+    cl = int(int(sizes.sum()) / d.nbytes * v)
+    ti = torch.from_numpy(idx).cuda()
+    k = idx.size
+    out = torch.empty((k, v), dtype=torch.int64, device="cuda")
+    wsb = lib.ibp_decompress_fetch_workspace_size(k, v, 8, 1)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        capi.check(lib.ibp_decompress_fetch(x.data_ptr(), n, v, 8, m.data_ptr(), b.data_ptr(),
+                                            bm.data_ptr(), ti.data_ptr(), k, cl, out.data_ptr(),
+                                            -1, -1, -1, ws.data_ptr(), wsb, st))
+    call()
+    torch.cuda.synchronize()
+    exact = bool(np.array_equal(out.cpu().numpy(), d[idx]))
+    for _ in range(warmup):
+        call()
+    torch.cuda.synchronize()
+    capi.check(lib.ibp_profile_enable(steps))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        call()
+    e1.record()
+    e1.synchronize()
+    buf = (ctypes.c_float * steps)()
+    got = lib.ibp_profile_take(buf, steps)
+    kms = float(np.mean(buf[:got])) if got else None
+    us = e0.elapsed_time(e1) * 1e3 / steps
+    comp_b = int(sizes[idx].sum())
+    # public API, one synchronised call at a time (what a latency-bound caller sees)
+    hidx = torch.from_numpy(idx).pin_memory()
+    res = torch.empty(v, dtype=torch.int64).pin_memory()
+    lat = []
+    for j in range(steps + warmup):
+        t0 = time.perf_counter()
+        o = ibp.decompress_fetch(x, m, b, bm, torch.device("cuda"), cl,
+                                 hidx.to("cuda", non_blocking=True))
+        res.copy_(o[-1], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        if j >= warmup:
+            lat.append((time.perf_counter() - t0) * 1e6)
+    ref = reference_module()
+    ref_us = None
+    if ref is not None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        ro = ref.decompress_fetch(x, m, b, bm, dev, cl, ti, None, None, None, None)
+        torch.cuda.synchronize()
+        ref_exact = bool(np.array_equal(ro.cpu().numpy(), d[idx]))
+        for _ in range(warmup):
+            ref.decompress_fetch(x, m, b, bm, dev, cl, ti, None, None, None, None)
+        torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record()
+        for _ in range(steps):
+            ref.decompress_fetch(x, m, b, bm, dev, cl, ti, None, None, None, None)
+        r1.record()
+        r1.synchronize()
+        ref_us = {"us_per_call": round(r0.elapsed_time(r1) * 1e3 / steps, 2),
+                  "bit_exact": ref_exact}
+    return {"workload": "plain_small: 16384 x 256 fp32 N(0,0.5^2), 5% rows N(0,100^2) -> int64 "
+                        "[16384 x 128] pinned host; threshold 0.9; 2048 distinct rows per call",
+            "us_per_call": round(us, 2), "GBps": round(k * v * 8 / us / 1e3, 3),
+            "kernel_us": None if kms is None else round(kms * 1e3, 2),
+            "kernel_pcie_frac": None if kms is None else round(comp_b / kms / 1e6 / pcie, 4),
+            "e2e_api_us": {"p50": round(float(np.percentile(lat, 50)), 2),
+                           "p99": round(float(np.percentile(lat, 99)), 2)},
+            "compressed_fraction": round(float(sizes.sum()) / d.nbytes, 4),
+            "setup_bit_exact_vs_oracle": setup_exact, "round_trip_bit_exact": exact,
+            "reference_gpu": ref_us, "steps": steps}
+
+
+def subconfig_line(config, extra_args, timeout):
+    """Run `bench.py --config <config>` in a child process (its own CUDA context and host
+    memory) and return its JSON line, or an error description."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--config", config] + extra_args
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, cwd=REPO)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout} s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"rc {r.returncode}: {r.stderr[-300:]}"}
+    return json.loads(lines[-1])
+
+
+def served_summary(line):
+    """The served-vs-per-call comparison of a served_mix line, rate by rate."""
+    if "rates" not in line:
+        return line
+    out = []
+    for e in line["rates"]:
+        srv, own = e["served"], e["per_request"]
+        ref = e.get("per_request_reference")
+        row = {"rate_per_s": e["rate_per_s"], "requests": e["requests"],
+               "served": srv, "per_request": own,
+               "served_beats_per_request": bool(srv["GBps"] >= own["GBps"]
+                                                 and srv["p99_ms"] <= own["p99_ms"])}
+        if ref is not None:
+            row["per_request_reference"] = ref
+            row["served_beats_reference_per_request"] = bool(
+                srv["GBps"] >= ref["GBps"] and srv["p99_ms"] <= ref["p99_ms"])
+        out.append(row)
+    return {"what": "continuous-batching server (hash-claimed batches) against one "
+                    "decompress_fetch per request, ours and the reference's, on Poisson "
+                    "arrivals; latency = completion - scheduled arrival",
+            "config": line.get("config"), "rates": out}
+
+
+def batched_summary(line):
+    """The batched line's headline numbers: graph-replayed batch, hashed and sorted batches,
+    one call per set (ours and the reference's), and the batch kernel's PCIe fraction."""
+    if "value" not in line:
+        return line
+    pick = lambda d: None if not isinstance(d, dict) else {  # noqa: E731
+        k: d[k] for k in ("value", "ms_per_step", "error") if k in d}
+    return {"metric": line["metric"], "value": line["value"], "unit": line["unit"],
+            "ms_per_step": line["ms_per_step"], "steps": line["steps"],
+            "hashed_batch": pick(line.get("hashed_batch")),
+            "sorted_batch": pick(line.get("sorted_batch")),
+            "per_call": pick(line.get("per_call")),
+            "reference_per_call": pick(line.get("reference_per_call")),
+            "kernel_pcie_frac": line.get("roofline", {}).get("frac"),
+            "compressed_fraction": line["config"].get("compressed_fraction")}
 
 
 def setup_vs_reference(torch, ibp, d, x_comp, m, b, bm, sizes):
@@ -350,8 +563,7 @@ def setup_vs_reference(torch, ibp, d, x_comp, m, b, bm, sizes):
     host-resident set, ours against the reference's (built from its sources for sm_100a),
     each timed on a fresh pinned copy of the uncompressed rows; the reference's masks, sizes,
     bitmask and compressed bytes are checked against ours bit for bit."""
-    import glob
-    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
+    ref = reference_module()
     y = torch.from_numpy(d).pin_memory()
 
     def run(pre, size, comp):
@@ -375,10 +587,7 @@ def setup_vs_reference(torch, ibp, d, x_comp, m, b, bm, sizes):
                   lambda t, mm, bb: ibp.compress_inplace(t, mm, bb))
     res = {"ours": ours, "what": "whole 1.2 GB host-resident set, fresh pinned copy each, "
                                  "wall time with device synchronisation"}
-    if mods:
-        sys.path.insert(0, os.path.dirname(mods[0]))
-        import ibp_cuda as ref
-        ref.print_debug(False)
+    if ref is not None:
         y.copy_(torch.from_numpy(d))
         theirs, (rm, rb, rsz, rbm) = run(
             lambda t: ref.preprocess(t, None),
@@ -397,13 +606,9 @@ def setup_vs_reference(torch, ibp, d, x_comp, m, b, bm, sizes):
 def reference_gpu(torch, comp, m, b, bm, comp_len, batches_dev, steps):
     """The reference extension (built from its sources for sm_100a, oracle/_ref) on the same
     compressed rows, through its own positional API; None when it is not built."""
-    import glob
-    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
-    if not mods:
+    ref = reference_module()
+    if ref is None:
         return None
-    sys.path.insert(0, os.path.dirname(mods[0]))
-    import ibp_cuda as ref
-    ref.print_debug(False)
     dev = torch.device("cuda")
     for k in range(3):
         ref.decompress_fetch(comp, m, b, bm, dev, comp_len, batches_dev[k % len(batches_dev)],
@@ -548,13 +753,9 @@ def reference_per_call(torch, sets, variants, outs, step_bytes, arrays, warmup, 
     the way its callers do: one call per tensor set per step, on the same compressed sets,
     index arrays and output tensors; None when the reference is not built.  Every output of
     the first pass over the request variants is checked against the source rows."""
-    import glob
-    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
-    if not mods:
+    ref = reference_module()
+    if ref is None:
         return None
-    sys.path.insert(0, os.path.dirname(mods[0]))
-    import ibp_cuda as ref
-    ref.print_debug(False)
     # the reference compares the output tensor's device with this one, index included
     dev = torch.device("cuda", torch.cuda.current_device())
 
@@ -599,13 +800,9 @@ def kmeans_vs_reference(torch, ibp, arrays):
     initial centroid rows are used by both (the reference's std::random_shuffle with the
     process's rand() state, restated by ours); the reference's assignment races on ties, so
     the masks are not compared here (the tests pin them on tie-free data)."""
-    import glob
-    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
-    if not mods:
+    ref = reference_module()
+    if ref is None:
         return None
-    sys.path.insert(0, os.path.dirname(mods[0]))
-    import ibp_cuda as ref
-    ref.print_debug(False)
     small = sorted(arrays, key=lambda a: a.shape[0])[:3]
     views = [torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).pin_memory() for a in small]
     res = {"rows": [int(a.shape[0]) for a in small], "words": 64}
@@ -758,6 +955,26 @@ def run_batched(args):
     s1.record()
     s1.synchronize()
     sms = s0.elapsed_time(s1)
+    # de-duplicating batch by hash claims inside the fetch (ibp_batch_fetch_hashed)
+    for reqs, o in zip(variants, outs):
+        bf.fetch(reqs, o, dedup="hash")
+        torch.cuda.synchronize()
+        for (sid, idx, first, count), oo in zip(reqs, o):
+            want = arrays[sid][idx.cpu().numpy()] if idx is not None else arrays[sid][first:first + count]
+            assert np.array_equal(oo.cpu().numpy(), want), "hashed batched fetch mismatch"
+    for k in range(args.warmup):
+        bf.fetch(variants[k % len(variants)], outs[k % len(variants)], dedup="hash")
+    torch.cuda.synchronize()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record()
+    htot = 0
+    for k in range(args.steps):
+        j = k % len(variants)
+        bf.fetch(variants[j], outs[j], dedup="hash")
+        htot += step_bytes[j]
+    h1.record()
+    h1.synchronize()
+    hms = h0.elapsed_time(h1)
     ref_steps = min(args.steps, 100)
     try:
         ref_call = reference_per_call(torch, sets, variants, outs, step_bytes, arrays,
@@ -792,6 +1009,10 @@ def run_batched(args):
                          "ms_per_step": round(sms / args.steps, 4),
                          "what": "one ibp_batch_fetch_sorted per step (device sort, repeats "
                                  "fetched once; not graph-captured)"},
+        "hashed_batch": {"value": round(htot / hms / 1e6, 3), "unit": "GB/s",
+                         "ms_per_step": round(hms / args.steps, 4),
+                         "what": "one ibp_batch_fetch_hashed per step (hash claims inside the "
+                                 "fetch, repeats copied on the device; not graph-captured)"},
         "roofline": {"bound": "pcie", "achieved": None if ach is None else round(ach, 3),
                      "peak": round(pcie, 3), "unit": "GB/s",
                      "frac": None if ach is None else round(ach / pcie, 4), "traffic": None,
@@ -891,18 +1112,12 @@ def run_rows(args, where):
     (12.5% .. 97%), decompressed whole (no index) onto the GPU.  Our decompress_fetch against
     the reference's own (built from its sources for sm_100a, its scripts' launch settings,
     impl 0) and the raw copy; CUDA-event times, every output checked bit for bit."""
-    import glob
     import torch
     torch.cuda.set_device(0)
     import invariantbitpacking_b200 as ibp
     from invariantbitpacking_b200 import _capi
     lib = _capi.lib
-    ref = None
-    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
-    if mods:
-        sys.path.insert(0, os.path.dirname(mods[0]))
-        import ibp_cuda as ref
-        ref.print_debug(False)
+    ref = reference_module()
     num = 100_000
     rng = np.random.default_rng(11)
     host = where == "host"
@@ -1049,13 +1264,8 @@ def run_served(args):
     reg = SetRegistry(sets)
     srv = Server(reg, arena_bytes=40 << 30, index_capacity=1 << 26, max_batch=256,
                  max_inflight=args.inflight, batch_bytes=args.batch_mb << 20)
-    import glob
-    ref = None
-    mods = glob.glob(os.path.join(REPO, "oracle", "_ref", "ibp_cuda*.so"))
-    if mods:  # the reference's decompress_fetch, built from its sources, as a third arm
-        sys.path.insert(0, os.path.dirname(mods[0]))
-        import ibp_cuda as ref
-        ref.print_debug(False)
+    srv.set_dedup(args.server_dedup)
+    ref = reference_module()  # the reference's decompress_fetch as a third arm (or None)
     rates = [float(r) for r in args.rates.split(",")]
     nreq = args.requests
     rng = np.random.default_rng(7)
@@ -1179,6 +1389,7 @@ def run_served(args):
         "config": {"workload": "served_mix: 8 pinned sets (~384 MB each), V in {64,128,256,512}, "
                                "Poisson arrivals, log-uniform [256, 262144] rows per request",
                    "arena_GB": 40, "max_batch": 256, "max_inflight": args.inflight,
+                   "server_dedup": args.server_dedup,
                    "batch_MiB": args.batch_mb,
                    "setup_s": round(setup_s, 1), "batches": st["batches"],
                    "bit_exact_checked_requests": checked},
@@ -1299,6 +1510,21 @@ def main():
     kms = kernel_ms(args.steps)
     ms = max_over_ranks(s0.elapsed_time(s1), ws)
     barrier(ws)
+    # the same measurement over a long region (1000 steps), with its own clock samples
+    LONG = 1000
+    with Clocks(torch.cuda.current_device()) as lclk:
+        l0e, l1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0e.record()
+        lrows = 0
+        for k in range(LONG):
+            lrows += engine_step(k)
+        l1e.record()
+        l1e.synchronize()
+    lms = max_over_ranks(l0e.elapsed_time(l1e), ws)
+    barrier(ws)
+    long_run = {"steps": LONG, "value": round((lrows * ws if not shard else sum(
+                    full_rows[k % len(batches)] for k in range(LONG))) * V * 8 / lms / 1e6, 3),
+                "ms_per_step": round(lms / LONG, 4), "clocks": lclk.summary()}
     job_rows = (sum(full_rows[k % len(batches)] for k in range(args.steps)) if shard
                 else rows * ws)
     value = job_rows * V * 8 / ms / 1e6  # GB/s, all ranks
@@ -1446,14 +1672,31 @@ def main():
     for r in range(4):
         engine_step(k400, xd)
     dms = kernel_ms(4)
+    # the whole call (claim pass, fetch, repeat copies) on the same batch
+    torch.cuda.synchronize()
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record()
+    for r in range(10):
+        engine_step(k400, xd)
+    w1.record()
+    w1.synchronize()
+    call_ms = w0.elapsed_time(w1) / 10
     nuniq = len(np.unique(batches[k400]))
     hbm_bytes = uniq_bytes[k400] + nuniq * V * 8
     hbm_gbs = hbm_bytes / (sum(dms) / len(dms)) / 1e6
+    call_bytes = uniq_bytes[k400] + len(batches[k400]) * V * 8
     hbm = {"bound": "hbm", "achieved": round(hbm_gbs, 1), "peak": hbm_peak, "unit": "GB/s",
            "frac": round(hbm_gbs / hbm_peak, 4), "traffic": None,
            "what": f"row-fetch kernel, device-resident copy of the set, 400k-row batch: "
                    f"compressed bytes read + decoded bytes written of {nuniq} distinct rows",
-           "peak_source": hbm_src}
+           "kernel_ms_per_launch": round(sum(dms) / len(dms), 4),
+           "peak_source": hbm_src,
+           "whole_call": {"ms": round(call_ms, 4),
+                          "achieved": round(call_bytes / call_ms / 1e6, 1),
+                          "frac": round(call_bytes / call_ms / 1e6 / hbm_peak, 4),
+                          "what": "the whole device-resident call (claim pass, fetch, repeat "
+                                  "copies): compressed bytes of the distinct rows read + all "
+                                  "400k output rows written, per call"}}
     del xd
 
     line = None
@@ -1483,21 +1726,14 @@ def main():
         if setup and "ours" in setup:
             sweep["gpu_compress_inplace"] = round(
                 d.nbytes / setup["ours"]["compress_inplace_ms"] / 1e6, 3)
-        nrows_avg = rows / args.steps
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "dtype": "int64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD,
-                       "rows": args.rows, "vec_words": V,
-                       "batches": BATCH_DESC,
-                       "avg_rows_per_step": nrows_avg, "comp_len_words": comp_len,
-                       "compressed_fraction": round(float(sizes_np.sum()) / d.nbytes, 4),
-                       "l2": "inputs larger than L2 (1.2 GB host set; 51-205 MB outputs)",
-                       "parallelism": (f"each batch split into {ws} contiguous shards"
-                                       if shard else f"{ws} independent replica(s)")},
+            "config": headline_config(args, ws, shard, args.steps, comp_len,
+                                      float(sizes_np.sum()) / d.nbytes),
             "e2e": {"value": round(e2e, 3), "unit": "GB/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps,
                     "what": "public API ibp.decompress_fetch; each step's index uploaded from "
@@ -1529,7 +1765,20 @@ def main():
             "setup_vs_reference": setup,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
+            "value_1000_steps": long_run,
         }
+        if not args.no_extras:
+            try:
+                line["plain_small"] = plain_small_summary(torch, ibp, lib, _capi, pcie,
+                                                          max(args.steps, 200), args.warmup)
+            except Exception as exc:  # reported, not fatal
+                line["plain_small"] = {"error": repr(exc)[:300]}
+            line["served_mix"] = served_summary(subconfig_line(
+                "served_mix", ["--rates", "2000,20000", "--requests", "150"], 900))
+            line["embedding_tables"] = batched_summary(subconfig_line(
+                "embedding_tables", ["--steps", "20", "--warmup", "3"], 900))
+            line["decoder_layer"] = batched_summary(subconfig_line(
+                "decoder_layer", ["--steps", "10", "--warmup", "3"], 900))
         print(json.dumps(line), flush=True)
     barrier(ws)
     if ws > 1:

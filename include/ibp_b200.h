@@ -4,7 +4,7 @@
  * Plain pointers and sizes only.  Every entry point replaces one function of the
  * reference's PyTorch extension `ibp_cuda` (src/ibp_api.cu:124-135); the comment on
  * each gives the reference file:line it replaces.  A foreign-function binding
- * (ctypes, cgo, JNI, N-API) binds these symbols directly; INTEGRATION.md shows one.
+ * (ctypes, cgo, JNI, N-API) binds these symbols directly.
  *
  * Conventions
  *  - dataset rows: `num_vecs` rows of `vec_size` words of `word_bytes` bytes, row stride
@@ -64,6 +64,15 @@ void ibp_set_debug(int on);
  * with few repeats are faster sorted.  No counterpart in the reference (it always sorts). */
 ibp_status ibp_set_fetch_dedup(int32_t mode);
 
+/* How long a repeated index of a hashed host-row fetch waits for the row of its first
+ * occurrence, which another warp of the same fetch decodes, process-wide: at most `polls`
+ * polls about 0.25 us apart (default 2^20, restored by -1).  A repeat that stops waiting
+ * decodes its own row from the source instead (one more read of that row) and sets bit 3 of
+ * the status word, so the output is the same whatever the limit; 0 makes every such repeat
+ * take that path at once, which tests use to exercise it.  No counterpart in the reference
+ * (it sorts and copies repeats after the fetch). */
+ibp_status ibp_set_repeat_wait_limit(int32_t polls);
+
 /* Profiling hooks (benchmarks): after ibp_profile_enable(cap), the next `cap` row-fetch
  * kernel launches (decompress_fetch, any thread) are bracketed by CUDA events on their
  * stream.  ibp_profile_take waits for them, writes their durations in milliseconds to ms[]
@@ -78,8 +87,9 @@ unsigned long long ibp_kernel_launch_count(void);
  * range; bit 1 = a row marked compressed has a bitmap whose stream would not fit the row
  * (the bitmask/mask do not belong to the data), and its output row was left untouched;
  * bit 2 = a sorted batch's request counts did not add up to its stated total_rows;
- * bit 3 = a repeated index gave up waiting (2^20 polls, a fraction of a second) for the row
- * of its first occurrence, and its output row was left untouched.
+ * bit 3 = a repeated index gave up waiting for the row of its first occurrence
+ * (ibp_set_repeat_wait_limit) and decoded its own row from the source instead: its output
+ * row is correct, the bit only reports the extra read.
  * Enqueues a copy on `stream` and waits for it (blocking). */
 ibp_status ibp_read_status(const void *workspace, int32_t *status, ibp_stream_t stream);
 
@@ -266,13 +276,30 @@ ibp_status ibp_batch_fetch_sorted(const void *registry, const ibp_request *reque
                                   int32_t num_requests, int64_t total_rows, void *workspace,
                                   size_t workspace_bytes, ibp_stream_t stream);
 
+/* De-duplicating batch without a sort: like ibp_batch_fetch_sorted (num_requests and total_rows
+ * host values, requests in device memory, bit 2 of the status word when the device counts
+ * disagree with total_rows), but each (set, row) of the batch is claimed in a hash table
+ * inside the fetch kernel, so a row listed several times -- in one request or across requests
+ * of the same set -- crosses the bus once, and its other output rows are copied on the device
+ * as soon as its first copy is written (the per-call ibp_decompress_fetch does the same for
+ * sparse host batches).  Each set gets row slots of its own length, so short rows keep
+ * several reads in flight per warp beside long ones.  Rows are fetched in request order, not
+ * row order.  Workspace: ibp_batch_fetch_hashed_workspace_size(max rows) bytes (32 per row);
+ * the status word is its first 4 bytes.  A repeat that waits too long for its row's first
+ * copy decodes its own (ibp_set_repeat_wait_limit). */
+size_t ibp_batch_fetch_hashed_workspace_size(int64_t max_total_rows);
+ibp_status ibp_batch_fetch_hashed(const void *registry, const ibp_request *requests,
+                                  int32_t num_requests, int64_t total_rows, void *workspace,
+                                  size_t workspace_bytes, ibp_stream_t stream);
+
 /* ---------------------------------------------------------------- serving
  * No counterpart in the reference (its callers issue one decompress_fetch per lookup).  A
  * continuous-batching server over a registry: clients submit requests from any thread; a
  * scheduler thread admits them in arrival order whenever their output fits the caller's
  * device arena, packs all admitted requests into one de-duplicating batched launch
- * (ibp_batch_fetch_sorted; a batch holds at most max(index_capacity, 2^20) rows, and a
- * single range request above that is fetched unsorted), and keeps up to max_inflight
+ * (ibp_batch_fetch_hashed, or ibp_batch_fetch_sorted after ibp_server_set_dedup(srv, 1); a
+ * batch holds at most max(index_capacity, 2^20) rows, and a single range request above that
+ * is fetched as listed), and keeps up to max_inflight
  * launches on the GPU, so requests arriving meanwhile join the next launch.  Buffers (index
  * staging rings of index_capacity entries, request tables, the sort workspace, a stream) are
  * allocated at creation only.  Timestamps are host steady-clock microseconds. */
@@ -300,6 +327,9 @@ ibp_status ibp_server_release(ibp_server *srv, int64_t id);
  * sort workspace's rows and 128 MiB.  Smaller batches finish early requests of a burst
  * sooner (lower p50); larger ones amortise per-launch cost. */
 ibp_status ibp_server_set_batch_limits(ibp_server *srv, int64_t max_rows, int64_t max_bytes);
+/* How later batches de-duplicate: 0 = hash claims inside the fetch (default), 1 = radix sort
+ * (rows then fetched in row order). */
+ibp_status ibp_server_set_dedup(ibp_server *srv, int32_t mode);
 /* stats[0..3] = batches launched, rows done, output bytes done, requests pending. */
 ibp_status ibp_server_stats(ibp_server *srv, int64_t *stats);
 /* Stop the scheduler after the in-flight batches finish and free the server's buffers. */
@@ -310,20 +340,28 @@ ibp_status ibp_server_destroy(ibp_server *srv);
  * (a host framework that owns every device byte and offers no allocation hook, an allocator
  * policy that forbids cudaMalloc on the request path, code that must not risk the implicit
  * device synchronisation of cudaMalloc/cudaFree).  Same arguments and results as
- * ibp_decompress_fetch without nblks/nthreads/impl/workspace; its scratch is a static 4 MiB
- * (4194304-byte) device array that the library reserves on every device that loads it, until
- * the process exits.  A call that needs more scratch than that
- * (ibp_decompress_fetch_workspace_size(...) > 4194304; roughly: more than ~100k index
- * entries) returns IBP_ERR_WORKSPACE before launching anything.  The first call on a
- * device looks the array's device address up (cudaGetSymbolAddress, with that device
- * current): make that first call before any stream capture on the device.  All calls share
- * the array, and calls whose GPU work overlaps (other streams, other threads) race on it:
- * serialise them.  Nothing is allocated or freed. */
+ * ibp_decompress_fetch without nblks/nthreads/impl/workspace; its scratch is a static
+ * IBP_NOALLOC_SCRATCH_BYTES (4 MiB) device array that the library reserves on every device
+ * that loads it, until the process exits.  A call fits exactly when
+ *     ibp_decompress_fetch_workspace_size(num_index, vec_size, word_bytes, num_index >= 0)
+ *         <= IBP_NOALLOC_SCRATCH_BYTES
+ * (about 40-48 bytes per index entry plus the column tables: ~90k entries of 64-word int64
+ * rows); a call that does not fit returns IBP_ERR_WORKSPACE before launching anything.  The
+ * first call in a CUDA context looks the array's device address up (cudaGetSymbolAddress,
+ * with that device current): make that first call before any stream capture on the device.
+ * All calls share the array, and calls whose GPU work overlaps (other streams, other
+ * threads) race on it: serialise them.  Nothing is allocated or freed. */
+#define IBP_NOALLOC_SCRATCH_BYTES 4194304
 ibp_status ibp_decompress_fetch_noalloc(const void *comp, int64_t num_vecs, int64_t vec_size,
                                         int word_bytes, const void *mask, const void *bitval,
                                         const int32_t *bitmask, const int64_t *index,
                                         int64_t num_index, int32_t comp_len, void *out,
                                         ibp_stream_t stream);
+/* Device status word of the last ibp_decompress_fetch_noalloc call on the current device
+ * (the same bits as ibp_read_status: out-of-range index, corrupt row, ...).  It is the
+ * first word of the shared static scratch, so read it before the next no-alloc call on the
+ * device.  Enqueues a copy on `stream` and waits for it (blocking). */
+ibp_status ibp_decompress_fetch_noalloc_status(int32_t *status, ibp_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -20,7 +20,8 @@ ibp_cuda.print_debug(False)
 __all__ = ["print_debug", "preprocess", "preprocess_kmeans", "get_compress_size",
            "get_single_compress_len", "compress_inplace", "compress", "compress_condensed",
            "decompress_fetch_condensed",
-           "decompress_fetch", "read_shared", "set_fetch_dedup", "ibp_cuda", "IBPError"]
+           "decompress_fetch", "read_shared", "set_fetch_dedup", "set_repeat_wait_limit",
+           "ibp_cuda", "IBPError"]
 
 
 def print_debug(flag):
@@ -68,16 +69,20 @@ def compress(dataset, mask, bitval, index_arr=None):
 
 
 def decompress_fetch(comp_dataset, mask, bitval, bitmask, device, comp_len=None,
-                     index_arr=None, nblks=None, nthds=None, imp=None, output_tensor=None):
+                     index_arr=None, nblks=None, nthds=None, imp=None, output_tensor=None, *,
+                     check=False):
+    """Decompressed rows (non-blocking).  check=True (keyword only; not in the reference) waits
+    for the call and raises RuntimeError when an index was out of range or a row could not be
+    decoded, instead of leaving those output rows unwritten."""
     return ibp_cuda.decompress_fetch(comp_dataset, mask, bitval, bitmask, device, comp_len,
-                                     index_arr, nblks, nthds, imp, output_tensor)
+                                     index_arr, nblks, nthds, imp, output_tensor, check=check)
 
 
 def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, device, index_arr=None,
-                               output_tensor=None):
+                               output_tensor=None, *, check=False):
     """Rows of the condensed layout (compress_condensed's words and byte offsets)."""
     return ibp_cuda.decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, device,
-                                               index_arr, output_tensor)
+                                               index_arr, output_tensor, check=check)
 
 
 def read_shared(filename, shape, dtype):
@@ -99,3 +104,12 @@ def set_fetch_dedup(mode):
         raise ValueError(f"set_fetch_dedup: mode must be one of {sorted(_DEDUP_MODES)} "
                          f"or 0/1/2, got {mode!r}")
     _capi.check(_capi.lib.ibp_set_fetch_dedup(int(m)))
+
+
+def set_repeat_wait_limit(polls=None):
+    """How many polls (~0.25 us apart) a repeated index of a hashed host-row fetch makes for
+    its first occurrence's row before decoding its own row from the source, process-wide
+    (None: the default, 2^20).  The output is the same whatever the limit; 0 sends every
+    such repeat down the decode-from-source path, which tests use to exercise it."""
+    from . import _capi
+    _capi.check(_capi.lib.ibp_set_repeat_wait_limit(-1 if polls is None else int(polls)))

@@ -29,6 +29,7 @@ SIGNATURES = {
     "ibp_set_debug": (None, [_INT]),
     "ibp_read_status": (_INT, [_P, _P, _P]),
     "ibp_set_fetch_dedup": (_INT, [_I32]),
+    "ibp_set_repeat_wait_limit": (_INT, [_I32]),
     "ibp_profile_enable": (_INT, [_I32]),
     "ibp_profile_take": (_I32, [_P, _I32]),
     "ibp_kernel_launch_count": (ctypes.c_ulonglong, []),
@@ -56,17 +57,24 @@ SIGNATURES = {
                                                _P, _P, _SZ, _P]),
     "ibp_batch_fetch_sorted_workspace_size": (_SZ, [_I64, _I32]),
     "ibp_batch_fetch_sorted": (_INT, [_P, _P, _I32, _I64, _P, _SZ, _P]),
+    "ibp_batch_fetch_hashed_workspace_size": (_SZ, [_I64]),
+    "ibp_batch_fetch_hashed": (_INT, [_P, _P, _I32, _I64, _P, _SZ, _P]),
     "ibp_server_create": (_INT, [_P, _P, _I32, _INT, _P, _SZ, _I64, _I32, _I32, _P]),
     "ibp_server_submit": (_INT, [_P, _I32, _P, _I64, _I64, _P]),
     "ibp_server_wait": (_INT, [_P, _I64, _I32, _P, _P]),
     "ibp_server_release": (_INT, [_P, _I64]),
     "ibp_server_cancel": (_INT, [_P, _I64]),
     "ibp_server_set_batch_limits": (_INT, [_P, _I64, _I64]),
+    "ibp_server_set_dedup": (_INT, [_P, _I32]),
     "ibp_server_stats": (_INT, [_P, _P]),
     "ibp_server_destroy": (_INT, [_P]),
     "ibp_decompress_fetch_noalloc": (_INT, [_P, _I64, _I64, _INT, _P, _P, _P, _P, _I64, _I32,
                                             _P, _P]),
+    "ibp_decompress_fetch_noalloc_status": (_INT, [_P, _P]),
 }
+
+# Bytes of the static scratch behind ibp_decompress_fetch_noalloc (IBP_NOALLOC_SCRATCH_BYTES)
+NOALLOC_SCRATCH_BYTES = 4194304
 
 
 class SetDesc(ctypes.Structure):

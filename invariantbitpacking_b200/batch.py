@@ -5,6 +5,7 @@
     outs = bf.fetch([(set_id, index_tensor_or_None, first, count), ...])
     bf.capture()     # later fetches replay one CUDA graph: copy of the request table + launch
     outs = bf.fetch(reqs, dedup=True)   # sort + de-duplicate each request's rows first
+    outs = bf.fetch(reqs, dedup="hash") # de-duplicate (set, row) by hash claims, no sort
 
 The request table (count + ibp_request records) is written into a pinned host buffer and
 copied to the device inside the captured work, so one graph serves any batch of up to
@@ -122,12 +123,27 @@ class BatchFetcher:
                                                 self.sort_ws.numel(), _stream()))
         self.last_ws = self.sort_ws
 
+    def _launch_hashed(self, b, nreq, rows):
+        need = _lib.ibp_batch_fetch_hashed_workspace_size(rows)
+        if self.sort_ws is None or self.sort_ws.numel() < need:
+            self.sort_ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+        d = self.dev[b]
+        d.copy_(self.host[b], non_blocking=True)
+        _capi.check(_lib.ibp_batch_fetch_hashed(self.reg.buf.data_ptr(), d.data_ptr() + _HDR, nreq,
+                                                rows, self.sort_ws.data_ptr(),
+                                                self.sort_ws.numel(), _stream()))
+        self.last_ws = self.sort_ws
+
     def fetch(self, requests, outs=None, dedup=False):
         """requests: (set id, int64 CUDA index or None, first row, row count) each.
 
-        dedup=True sorts each request's rows on the device and fetches a repeated row once
-        (ibp_batch_fetch_sorted); it runs outside the captured graphs, whose table shape is
+        dedup=True (or "sort") sorts each request's rows on the device and fetches a repeated
+        row once (ibp_batch_fetch_sorted); dedup="hash" claims each (set, row) in a hash table
+        inside the fetch instead (ibp_batch_fetch_hashed), which also shares rows between
+        requests of one set.  Both run outside the captured graphs, whose table shape is
         fixed at capture."""
+        if dedup not in (False, True, "sort", "hash"):
+            raise ValueError(f"dedup must be False, True, 'sort' or 'hash', got {dedup!r}")
         requests = [(s, (None if i is None else i.to(torch.int64)), f, c) for s, i, f, c in requests]
         if outs is None:
             outs = self.outputs_for(requests)
@@ -136,7 +152,11 @@ class BatchFetcher:
         self._write(b, requests, outs)
         if dedup:
             if requests:
-                self._launch_sorted(b, len(requests), sum(max(int(r[3]), 0) for r in requests))
+                rows = sum(max(int(r[3]), 0) for r in requests)
+                if dedup == "hash":
+                    self._launch_hashed(b, len(requests), rows)
+                else:
+                    self._launch_sorted(b, len(requests), rows)
         elif self.graphs is not None:
             self.last_ws = self.ws
             self.graphs[b].replay()

@@ -29,6 +29,7 @@ struct RegistryHeader {
     int64_t max_n;           // most rows of any set
     int32_t host_resident;   // set 0 lives in host memory
     int32_t ratio_bucket;    // mean first-read fraction of the rows, in tenths
+    int64_t max_slot_words;  // largest row slot any set needs (set_slot_words)
 };
 
 struct RequestDev {  // mirrors ibp_request
@@ -40,6 +41,20 @@ struct RequestDev {  // mirrors ibp_request
     void *out;
 };
 static_assert(sizeof(RequestDev) == sizeof(ibp_request), "request layout");
+
+// Shared-memory words of one row slot of a set: the row plus the two words the decoder
+// reads past the stream, in whole 16-byte blocks; rows over 256 words get slots for twice
+// their first read only (longer rows decode from their source), as in the per-call fetch.
+template <typename U>
+__host__ __device__ inline int64_t set_slot_words(int64_t v, int64_t first_words) {
+    constexpr int64_t per16 = 16 / sizeof(U);
+    int64_t w = v;
+    if (v > 256) {
+        const int64_t cap = 2 * first_words > 256 ? 2 * first_words : 256;
+        w = v < cap ? v : cap;
+    }
+    return (w + 2 + per16 - 1) / per16 * per16;
+}
 
 template <typename U>
 struct BatchArgs {
@@ -216,6 +231,8 @@ static ibp_status register_sets(const ibp_set_desc *sets, int nsets, void *reg, 
             return IBP_ERR_WORKSPACE;
         }
         h.max_v = std::max<int64_t>(h.max_v, d.vec_size);
+        h.max_slot_words =
+            std::max<int64_t>(h.max_slot_words, set_slot_words<U>(d.vec_size, s.first_words));
         h.max_n = std::max<int64_t>(h.max_n, d.num_vecs);
         ratio += d.vec_size > 0 ? (double)s.first_words / (double)d.vec_size : 1.0;
         if (d.vec_size > 0) IBP_RET(build_tables<U>((const U *)d.mask, (const U *)d.bitval, d.vec_size, s.t, st));
@@ -594,6 +611,174 @@ static ibp_status launch_sorted(const void *reg, const RegistryHeader &h, const 
     return IBP_OK;
 }
 
+// ------------------------------------------------------------------ hashed batches
+// A de-duplicating batch without a sort: every unit of a request claims its rows in a hash
+// table keyed by (set, row) before fetching them, so a row listed several times -- in one
+// request or across requests of the same set -- crosses the bus once; repeats copy the output
+// row of their row's first claim inside the same kernel once it is published (claim_chunk /
+// settle_chunk), behind the other warps' host reads.  Each set gets the row slots of its own
+// row length out of a warp's shared memory (so short rows keep kRowsInFlight rows in flight
+// beside long ones), and sets of at most 64 words decode from register tables.
+template <typename U>
+struct HashedArgs {
+    const RowSet<U> *sets;
+    int32_t nsets;
+    const RequestDev *reqs;
+    int32_t nreq;
+    int64_t total;            // the caller's row total (the table was sized for it)
+    unsigned long long *work;
+    int32_t *status;
+    ClaimTable claims;
+    int64_t warp_words;       // shared-memory words of row slots per warp
+};
+
+constexpr int kSetKeyShift = 40;  // claim key: (set << 40) | row
+
+template <typename U>
+__global__ void __launch_bounds__(256, 2) batch_fetch_hashed_kernel(HashedArgs<U> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int64_t *prefix = reinterpret_cast<int64_t *>(smem);
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    U *slots = reinterpret_cast<U *>(smem + batch_head_bytes(a.nreq)) + (int64_t)warp * a.warp_words;
+    int64_t *park = reinterpret_cast<int64_t *>(reinterpret_cast<U *>(smem + batch_head_bytes(a.nreq)) +
+                                                (int64_t)nwarps * a.warp_words) +
+                    warp * 64;
+    const int upos = unit_prefix(a.reqs, a.nreq, prefix, prefix + a.nreq + 1);
+    const int lane = threadIdx.x & 31;
+    const int64_t total_units = prefix[a.nreq];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int64_t rows = 0;
+        for (int r = 0; r < a.nreq; ++r) rows += max(a.reqs[r].count, (int64_t)0);
+        if (rows != a.total) atomicOr(a.status, kStatusBadTable);
+    }
+    LaneTables<U, 2> lt;  // register tables of the current set when its rows are short
+    LaneTables<U, 0> lt0;
+    int cur_set = -1;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(a.work, 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if ((int64_t)u >= total_units) break;
+        const int r = unit_owner(prefix, a.nreq, (int64_t)u);
+        const RequestDev rq = a.reqs[r];
+        const int64_t k = ((int64_t)u - prefix[r]) * upos + lane;
+        if (rq.set < 0 || rq.set >= a.nsets) {
+            if (lane == 0) atomicOr(a.status, kStatusBadIndex);
+            continue;
+        }
+        const RowSet<U> &s = a.sets[rq.set];
+        const bool small = s.v <= 64;
+        if (small && rq.set != cur_set) {
+            lt.load(s.t, s.v);
+            cur_set = rq.set;
+        }
+        const bool valid = lane < upos && k < rq.count;
+        const int64_t key = valid ? (rq.index ? rq.index[k] : rq.first + k) : -1;
+        const bool bad = valid && (key < 0 || key >= s.n);
+        if (bad) atomicOr(a.status, kStatusBadIndex);
+        bool head = valid && !bad;
+        U *orow = reinterpret_cast<U *>(rq.out) + (head ? k : 0) * s.v;
+        const bool rep =
+            claim_chunk(a.claims, park, ((int64_t)rq.set << kSetKeyShift) | key, head, orow);
+        const int64_t sw = set_slot_words<U>(s.v, s.first_words);
+        const int ns = (int)min((int64_t)kRowsInFlight, a.warp_words / sw);
+        bool fetch_lane = head;
+        for (int pass = 0;; ++pass) {
+            const bool packed =
+                fetch_lane && ((__ldg(&s.bitmask[key >> 5]) >> (key & 31)) & 1);
+            if (small)
+                fetch_heads<U, 2>(s, lt, slots, ns, sw, key, orow, fetch_lane, packed, a.status);
+            else
+                fetch_heads<U, 0>(s, lt0, slots, ns, sw, key, orow, fetch_lane, packed, a.status);
+            if (pass > 0) break;
+            fetch_lane = settle_chunk<U>(a.claims, park, rep, s.v, a.status);
+            if (!__any_sync(0xffffffffu, fetch_lane)) break;
+        }
+    }
+}
+
+// Slots of the hashed batch's claim table for `rows` positions (load factor at most 1/2).
+static int64_t batch_hash_slots(int64_t rows) {
+    return std::max<int64_t>(64, (2 * rows + 63) / 64 * 64);
+}
+
+static size_t hashed_workspace(int64_t rows) {
+    Sizer z;
+    z.take<char>(kStatusBytes);
+    z.take<int64_t>((size_t)batch_hash_slots(rows));
+    z.take<int64_t>((size_t)batch_hash_slots(rows));
+    return z.total();
+}
+
+template <typename U>
+static ibp_status launch_hashed(const void *reg, const RegistryHeader &h, const RequestDev *dreqs,
+                                int nreq, int64_t rows, void *ws, size_t ws_bytes, Shape sh,
+                                cudaStream_t st) {
+    const size_t need = hashed_workspace(rows);
+    if (!ws || ws_bytes < need) {
+        set_error("batch_fetch_hashed: workspace of %zu bytes is below the required %zu for %lld "
+                  "rows", ws_bytes, need, (long long)rows);
+        return IBP_ERR_WORKSPACE;
+    }
+    if (h.nsets > (1 << (62 - kSetKeyShift)) || h.max_n > ((int64_t)1 << kSetKeyShift)) {
+        set_error("batch_fetch_hashed: %d sets of up to %lld rows exceed the claim key",
+                  h.nsets, (long long)h.max_n);
+        return IBP_ERR_UNSUPPORTED;
+    }
+    Carver c{(char *)reg, 0, (size_t)-1};
+    c.take<RegistryHeader>(1);
+    const RowSet<U> *sets = c.take<RowSet<U>>((size_t)h.nsets);
+    Carver w{(char *)ws, 0, ws_bytes};
+    int32_t *status = w.take<int32_t>(kStatusBytes / 4);
+    const int64_t hs = batch_hash_slots(rows);
+    int64_t *hkeys = w.take<int64_t>((size_t)hs);
+    int64_t *hrows = w.take<int64_t>((size_t)hs);
+    IBP_CUDA(cudaMemsetAsync(status, 0, 128, st));
+    // keys -1 (empty), rows -1 (unpublished)
+    IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, (char *)(hrows + hs) - (char *)hkeys, st));
+    HashedArgs<U> a{};
+    a.sets = sets;
+    a.nsets = h.nsets;
+    a.reqs = dreqs;
+    a.nreq = nreq;
+    a.total = rows;
+    a.work = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 64);
+    a.status = status;
+    a.claims = ClaimTable{hkeys, hrows, hs, repeat_wait_polls()};
+    // a warp's row slots: kRowsInFlight of the largest set's, within ~96 KB per block (at
+    // least one), so the short rows of other sets get up to kRowsInFlight slots of their own
+    const size_t head = batch_head_bytes(nreq);
+    const size_t park_bytes = 64 * sizeof(int64_t);
+    int threads = sh.threads;
+    const int64_t want = h.max_slot_words * std::max(1, std::min(sh.slots, kRowsInFlight));
+    int64_t warp_words = want;
+    const int maxs = device_max_smem_optin();
+    auto smem_of = [&](int64_t ww, int t) {
+        return head + ((size_t)ww * sizeof(U) + park_bytes) * (size_t)(t / 32);
+    };
+    while (warp_words > h.max_slot_words && smem_of(warp_words, threads) > 96 * 1024)
+        warp_words -= h.max_slot_words;
+    while (threads > 32 && smem_of(warp_words, threads) > (size_t)maxs) threads -= 32;
+    const size_t smem = smem_of(warp_words, threads);
+    if ((int64_t)smem > maxs) {
+        set_error("batch_fetch_hashed: %d requests and rows of %lld words do not fit shared "
+                  "memory", nreq, (long long)h.max_v);
+        return IBP_ERR_UNSUPPORTED;
+    }
+    a.warp_words = warp_words;
+    auto kern = batch_fetch_hashed_kernel<U>;
+    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    if (per_sm < 1) per_sm = 1;
+    if (sh.occupancy > 0 && sh.occupancy < per_sm) per_sm = sh.occupancy;
+    const int pslot = profile_begin(st);
+    kern<<<device_sm_count() * per_sm, threads, smem, st>>>(a);
+    IBP_LAUNCHED("batch_fetch_hashed_kernel");
+    profile_end(pslot, st);
+    return IBP_OK;
+}
+
 }  // namespace ibp200
 
 using namespace ibp200;
@@ -751,6 +936,42 @@ ibp_status ibp_batch_fetch_sorted(const void *registry, const ibp_request *reque
         return launch_sorted<uint64_t>(registry, h, dreqs, num_requests, total_rows, workspace,
                                        workspace_bytes, sh, st);
     return launch_sorted<uint32_t>(registry, h, dreqs, num_requests, total_rows, workspace,
+                                   workspace_bytes, sh, st);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+size_t ibp_batch_fetch_hashed_workspace_size(int64_t max_total_rows) {
+    if (max_total_rows < 0 || max_total_rows > INT32_MAX) return 0;
+    return hashed_workspace(max_total_rows);
+}
+
+ibp_status ibp_batch_fetch_hashed(const void *registry, const ibp_request *requests,
+                                  int32_t num_requests, int64_t total_rows, void *workspace,
+                                  size_t workspace_bytes, ibp_stream_t stream) {
+    clear_error();
+    IBP_RANGE("ibp_batch_fetch_hashed");
+    IBP_ARG(registry && requests, "batch_fetch_hashed: null argument");
+    IBP_ARG(num_requests > 0 && num_requests <= 8192,
+            "batch_fetch_hashed: num_requests must be 1..8192");
+    IBP_ARG(total_rows >= 0 && total_rows <= INT32_MAX,
+            "batch_fetch_hashed: total_rows must be 0..2^31-1");
+    RegistryHeader h{};
+    IBP_RET(read_header(registry, h));
+    Shape sh;
+    {
+        std::lock_guard<std::mutex> g(g_shape_mu);
+        auto it = g_shapes.find(ShapeKey{h.word_bytes, h.max_v, h.ratio_bucket, h.host_resident});
+        if (it != g_shapes.end()) sh = it->second;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const RequestDev *dreqs = reinterpret_cast<const RequestDev *>(requests);
+    if (h.word_bytes == 8)
+        return launch_hashed<uint64_t>(registry, h, dreqs, num_requests, total_rows, workspace,
+                                       workspace_bytes, sh, st);
+    return launch_hashed<uint32_t>(registry, h, dreqs, num_requests, total_rows, workspace,
                                    workspace_bytes, sh, st);
 }
 

@@ -32,6 +32,10 @@ static Profiler &profiler() {
 static std::atomic<int> g_dedup_mode{0};
 int fetch_dedup_mode() { return g_dedup_mode.load(std::memory_order_relaxed); }
 
+constexpr int kDefaultRepeatWaitPolls = 1 << 20;  // ~0.25 s of polls 0.25 us apart
+static std::atomic<int> g_repeat_wait_polls{kDefaultRepeatWaitPolls};
+int repeat_wait_polls() { return g_repeat_wait_polls.load(std::memory_order_relaxed); }
+
 int profile_begin(cudaStream_t st) {
     Profiler &p = profiler();
     std::lock_guard<std::mutex> g(p.mu);
@@ -175,6 +179,13 @@ ibp_status ibp_set_fetch_dedup(int32_t mode) {
     clear_error();
     IBP_ARG(mode >= 0 && mode <= 2, "set_fetch_dedup: mode must be 0 (auto), 1 (sort) or 2 (hash)");
     g_dedup_mode.store(mode);
+    return IBP_OK;
+}
+
+ibp_status ibp_set_repeat_wait_limit(int32_t polls) {
+    clear_error();
+    IBP_ARG(polls >= -1, "set_repeat_wait_limit: polls must be >= 0, or -1 for the default");
+    g_repeat_wait_polls.store(polls < 0 ? kDefaultRepeatWaitPolls : polls);
     return IBP_OK;
 }
 

@@ -33,6 +33,7 @@ struct NvtxRange {
 
 int profile_begin(cudaStream_t st);
 int fetch_dedup_mode();  // ibp_set_fetch_dedup: 0 auto, 1 sort, 2 hash
+int repeat_wait_polls();  // ibp_set_repeat_wait_limit
 void profile_end(int slot, cudaStream_t st);
 
 #define IBP_DPRINTF(...)                       \

@@ -60,118 +60,21 @@ struct FetchArgs {
     int upos;             // positions per chunk the grid was sized for (unit_positions)
     int gmax;             // largest chunk a warp takes (positions); 0: its row slots
     bool async_rows;      // rows in device memory: first reads as asynchronous copies
-    int64_t *hkeys;       // in-fetch claims: open-addressing table of rows (-1 = empty) ...
-    int64_t *hpos;        // ... and, once its row is written, the position that claimed each
-                          // with kRowDone set (-1 before; nullptr: no claims); repeats are
-                          // copied inside the fetch
-    int64_t hslots;       // the table's slots
+    bool device_rows;     // rows in device memory
+    ClaimTable claims;    // in-fetch claims (keys == nullptr: none); repeats are copied
+                          // inside the fetch
     const int64_t *list;  // positions to fetch (claimed heads), or nullptr: all positions
     const unsigned long long *list_len;  // entries of `list` (device)
 };
 
 // ------------------------------------------------------------------ hashed dedup
-// The first position to claim a row in the table fetches it; later ones are repeats.  The
-// table has at least twice as many slots as positions, so linear probing ends quickly.
-__device__ __forceinline__ uint64_t row_hash(int64_t key, int64_t slots) {
-    return __umul64hi((uint64_t)key * 0x9E3779B97F4A7C15ull, (uint64_t)slots);
-}
-
-// The table slot holding `key` after this call: claimed by it (`won`) or by an earlier one;
-// -1 when the table is full (it never is: it has twice as many slots as positions).
-__device__ __forceinline__ int64_t hash_claim_slot(int64_t *keys, int64_t slots, int64_t key,
-                                                   bool &won) {
-    won = false;
-    uint64_t h = row_hash(key, slots);
-    for (int64_t probe = 0; probe < slots; ++probe) {
-        // a plain read first: a row already claimed (hot rows of a skewed batch) costs no
-        // atomic, so repeats do not queue on one address
-        const int64_t cur = *reinterpret_cast<volatile int64_t *>(keys + h);
-        if (cur == key) return (int64_t)h;
-        if (cur == -1) {
-            const unsigned long long old = atomicCAS(
-                reinterpret_cast<unsigned long long *>(keys + h), ~0ull, (unsigned long long)key);
-            if (old == ~0ull) {
-                won = true;
-                return (int64_t)h;
-            }
-            if ((int64_t)old == key) return (int64_t)h;
-        }
-        h = h + 1 == (uint64_t)slots ? 0 : h + 1;
-    }
-    return -1;
-}
-
+// (row_hash, hash_claim_slot and the in-fetch claim helpers are in ibp_fetch.cuh)
 __device__ __forceinline__ bool hash_claim(int64_t *keys, int64_t *pos, int64_t slots,
                                            int64_t key, int64_t k) {
     bool won;
     const int64_t h = hash_claim_slot(keys, slots, key, won);
     if (won) pos[h] = k;
     return won;
-}
-
-// In-fetch claims publish each claimed row's position with this bit once the row is written.
-constexpr int64_t kRowDone = 1ll << 62;
-constexpr int kRepeatWaitLimit = 1 << 20;  // polls (~0.25 us apart) before a repeat gives up
-
-__device__ __forceinline__ int64_t load_acquire(const int64_t *p) {
-    int64_t x;
-    asm volatile("ld.acquire.gpu.global.s64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
-    return x;
-}
-
-__device__ __forceinline__ void store_release(int64_t *p, int64_t x) {
-    asm volatile("st.release.gpu.global.s64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
-}
-
-// Copy rows src -> dst for the lanes of `dm` (each lane's src/dst), four rows at a time: all
-// four rows' loads before any store (16-byte moves when the rows are aligned), so the loads'
-// latencies overlap.  Sources are read through L2 (other SMs may have just written them).
-template <typename U>
-__device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_row, int64_t v,
-                                          bool vec_rows) {
-    constexpr int R = 4;
-    const int lane = threadIdx.x & 31;
-    while (dm) {
-        const U *src[R];
-        U *dst[R];
-        int cnt = 0;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            src[r] = src_row;
-            dst[r] = dst_row;
-            if (dm) {
-                const int j = __ffs(dm) - 1;
-                dm &= dm - 1;
-                src[r] = reinterpret_cast<const U *>(__shfl_sync(
-                    0xffffffffu, reinterpret_cast<unsigned long long>(src_row), j));
-                dst[r] = reinterpret_cast<U *>(__shfl_sync(
-                    0xffffffffu, reinterpret_cast<unsigned long long>(dst_row), j));
-                cnt = r + 1;
-            }
-        }
-        if (vec_rows) {
-            const int64_t n16 = v * (int64_t)sizeof(U) / 16;
-            for (int64_t q = lane; q < n16; q += 32) {
-                uint4 t[R];
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r < cnt) t[r] = __ldcg(reinterpret_cast<const uint4 *>(src[r]) + q);
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
-            }
-        } else {
-            for (int64_t q = lane; q < v; q += 32) {
-                U t[R];
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r < cnt) t[r] = __ldcg(src[r] + q);
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r < cnt) dst[r][q] = t[r];
-            }
-        }
-    }
 }
 
 __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
@@ -295,80 +198,212 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
         const bool bad = head && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         head = head && !bad;
-        // in-fetch claims: one claim per distinct row of the chunk (its lowest lane); the
-        // other lanes of that row, and the lanes whose row was claimed earlier, are repeats.
-        // Each lane parks its table slot (kRowDone set: it claimed the row) and position in
-        // shared memory until its chunk's rows are fetched, which keeps them out of the
-        // registers the fetch needs.
+        // in-fetch claims: one claim per distinct row of the chunk; the other lanes of that
+        // row, and the lanes whose row was claimed earlier, are repeats
+        const bool claims = kClaims && a.claims.keys;
         bool rep = false;
-        if (kClaims && a.hkeys) {
-            const unsigned same = __match_any_sync(0xffffffffu, head ? key : (int64_t)-1);
-            const int first = __ffs(same) - 1;
-            bool won = false;
-            int64_t slot = -1;
-            if (head && first == lane) slot = hash_claim_slot(a.hkeys, a.hslots, key, won);
-            slot = __shfl_sync(0xffffffffu, slot, first);
-            rep = head && !won && slot >= 0;
-            head = won;
-            claim[lane] = head ? slot | kRowDone : (rep ? slot : -1);
-            claim[32 + lane] = k;
+        const bool out_row = head;  // lanes with an output row (heads before claiming)
+        U *orow = a.out + (out_row ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
+        if (claims) rep = claim_chunk(a.claims, claim, key, head, orow);
+        // pass 0 fetches the chunk's claimed (or, without claims, all) rows; pass 1, which
+        // only in-fetch claims need, fetches the rows of repeats that gave up waiting for
+        // their first occurrence, from their source like any other row
+        bool fetch_lane = head;
+        for (int pass = 0;; ++pass) {
+            if constexpr (EXACT) {
+                fetch_heads_exact<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow,
+                                         fetch_lane, a.status);
+            } else {
+                const bool packed = fetch_lane && !a.raw_only &&
+                                    ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1);
+                if constexpr (ASYNC)
+                    fetch_heads_async<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow,
+                                             fetch_lane, packed, a.status);
+                else
+                    fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow,
+                                       fetch_lane, packed, a.status);
+            }
+            if (!claims || pass > 0) break;
+            fetch_lane = settle_chunk<U>(a.claims, claim, rep, a.s.v, a.status);
+            if (!__any_sync(0xffffffffu, fetch_lane)) break;
         }
-        U *orow = a.out + (head || rep ? (a.pos ? a.pos[k] : k) : 0) * a.s.v;
-        if constexpr (EXACT) {
-            fetch_heads_exact<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
-                                     a.status);
-        } else {
-            const bool packed =
-                head && !a.raw_only && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1);
-            if constexpr (ASYNC)
-                fetch_heads_async<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
-                                         packed, a.status);
-            else
-                fetch_heads<U, NC>(a.s, lt, slots, a.slots, a.slot_words, key, orow, head,
-                                   packed, a.status);
+    }
+}
+
+// ------------------------------------------------------------------ HBM rows of <= 64 words
+// Rows in device memory are not bound by a link but by the instructions around the decode,
+// so this kernel keeps per-row bookkeeping to a minimum: a warp takes 32 listed rows (the
+// claim pass's distinct rows, or rows p .. p+31 of an unindexed fetch), parks their keys and
+// output rows in shared memory, and copies groups of G whole rows (one 16-byte cp.async per
+// lane and row; rows must be 16-byte aligned) into one of two shared buffers while it
+// decodes the previous group from the other.  A group's prefix sums are issued together;
+// the row's stream length falls out of them (no separate length pass, no tail reads), and
+// stream offsets are 32-bit.
+template <typename U>
+__device__ __forceinline__ U stream_bits(const U *words, uint32_t s, int L) {
+    constexpr int W = 8 * sizeof(U);
+    const uint32_t q = s / W;
+    const int r = (int)(s % W);
+    const U hi = words[q], lo = words[q + 1];
+    // (lo >> 1) >> (W - 1 - r) is lo >> (W - r) for r >= 1 and 0 for r == 0
+    const U win = (U)((hi << r) | ((lo >> 1) >> (W - 1 - r)));
+    return L == 0 ? (U)0 : (U)(win >> (W - L));
+}
+
+template <typename U, int NC, int G>
+__device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int sw, int r0,
+                                                 int rows, unsigned okm, unsigned pm, int v,
+                                                 int mw, const LaneTables<U, NC> &lt,
+                                                 U *const *mout, int32_t *status) {
+    constexpr int W = 8 * sizeof(U);
+    const int lane = threadIdx.x & 31;
+    uint32_t incl[G][NC];
+    unsigned cjm = 0;  // bit q * NC + c: this lane's column of chunk c in row q is compressible
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+        const int r = r0 + q;
+        const bool pk = r < rows && ((pm >> r) & 1);
+        const uint32_t *units = reinterpret_cast<const uint32_t *>(buf + q * sw);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const bool in = 32 * c + lane < v;
+            const bool cj = pk && in && ((units[c] >> lane) & 1u);
+            cjm |= (unsigned)cj << (q * NC + c);
+            incl[q][c] = (pk && in) ? (cj ? (uint32_t)lt.nb[c] : (uint32_t)W) : 0u;
         }
-        if (kClaims && a.hkeys) {
-            // publish this chunk's rows (every lane's stores are ordered before the release
-            // by the warp barrier), then copy its repeats once their rows are published.  A
-            // warp waits only after publishing all of its own claims, so every row waited
-            // on belongs to a warp that is still fetching and waits on nothing.
-            __syncwarp();
-            const int64_t cw = claim[lane];
-            const int64_t kk = claim[32 + lane];
-            const bool own = cw >= 0 && (cw & kRowDone);
-            const bool rep = cw >= 0 && !own;
-            const int64_t slot = cw & ~kRowDone;
-            if (own) store_release(a.hpos + slot, kk | kRowDone);
-            if (__any_sync(0xffffffffu, rep)) {
-                int64_t src = -1;
-                // once any wait has given up, later ones make a single check (lane 0 reads
-                // the status word, so that every lane has the same bound)
-                int limit = 0;
-                if (lane == 0)
-                    limit = (*reinterpret_cast<volatile int32_t *>(a.status) & kStatusWaitTimeout)
-                                ? 0
-                                : kRepeatWaitLimit;
-                limit = __shfl_sync(0xffffffffu, limit, 0);
-                for (int it = 0;; ++it) {
-                    if (rep && src < 0) {
-                        const int64_t hv = load_acquire(a.hpos + slot);
-                        if (hv >= 0 && (hv & kRowDone)) src = hv & ~kRowDone;
-                    }
-                    if (__all_sync(0xffffffffu, !rep || src >= 0)) break;
-                    if (it >= limit) {
-                        if (rep && src < 0) atomicOr(a.status, kStatusWaitTimeout);
-                        break;
-                    }
-                    __nanosleep(256);
-                }
-                const bool go = rep && src >= 0;
-                copy_rows<U>(__ballot_sync(0xffffffffu, go), a.out + (go ? src : 0) * a.s.v,
-                             a.out + (go ? kk : 0) * a.s.v, a.s.v,
-                             ((a.s.v * (int64_t)sizeof(U)) & 15) == 0 &&
-                                 (((uintptr_t)a.out) & 15) == 0);
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl[q][c], off);
+                if (lane >= off) incl[q][c] += y;
             }
         }
     }
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+        const int r = r0 + q;
+        if (r >= rows || !((okm >> r) & 1)) continue;
+        U *o = mout[r];
+        const U *row = buf + q * sw;
+        if (!((pm >> r) & 1)) {  // stored raw
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (32 * c + lane < v) o[32 * c + lane] = row[32 * c + lane];
+            continue;
+        }
+        const uint32_t t0 = __shfl_sync(0xffffffffu, incl[q][0], 31);
+        uint32_t tot = t0;
+        if (NC > 1) tot += __shfl_sync(0xffffffffu, incl[q][NC - 1], 31);
+        if (mw + (int)((tot + W - 1) / W) >= v) {
+            // a bitmap claiming a stream as long as the raw row cannot come from this mask:
+            // report it and leave the output row alone
+            if (lane == 0) atomicOr(status, kStatusCorruptRow);
+            continue;
+        }
+        const U *stream = row + mw;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int j = 32 * c + lane;
+            if (j < v) {
+                const bool cj = (cjm >> (q * NC + c)) & 1u;
+                const int L = cj ? (int)lt.nb[c] : W;
+                const U y = stream_bits<U>(stream, (c ? t0 : 0u) + incl[q][c] - (uint32_t)L, L);
+                o[j] = cj ? (U)(lt.bv[c] | scatter_regs<U>(y, (U)~lt.m[c], lt.mv[c])) : y;
+            }
+        }
+    }
+}
+
+template <typename U, int NC, int G>
+__global__ void __launch_bounds__(256, 3) hbm_rows_kernel(FetchArgs<U> a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int per16 = 16 / sizeof(U);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t *mkey = reinterpret_cast<int64_t *>(smem) + warp * 64;
+    U **mout = reinterpret_cast<U **>(mkey + 32);
+    const int sw = (int)a.slot_words;
+    U *bufs = reinterpret_cast<U *>(smem + (blockDim.x >> 5) * 512) + (int64_t)warp * 2 * G * sw;
+    LaneTables<U, NC> lt;
+    lt.load(a.s.t, a.s.v);
+    const int v = (int)a.s.v, mw = (int)a.s.mw;
+    const int nq16 = v / per16;  // 16-byte blocks of a row (<= 32)
+    const int64_t nrows = a.list ? (int64_t)*a.list_len : a.nrows;
+    for (;;) {
+        unsigned long long c0 = 0;
+        if (lane == 0) c0 = atomicAdd(a.work, 32ull);
+        const int64_t p0 = (int64_t)__shfl_sync(0xffffffffu, c0, 0);
+        if (p0 >= nrows) break;
+        const int rows = (int)min((int64_t)32, nrows - p0);
+        const bool valid = lane < rows;
+        const int64_t k = valid ? (a.list ? a.list[p0 + lane] : p0 + lane) : 0;
+        const int64_t key = valid ? (a.keys ? a.keys[k] : k) : 0;
+        const bool bad = valid && (key < 0 || key >= a.s.n);
+        if (bad) atomicOr(a.status, kStatusBadIndex);
+        const bool ok = valid && !bad;
+        const unsigned okm = __ballot_sync(0xffffffffu, ok);
+        const unsigned pm = __ballot_sync(
+            0xffffffffu, ok && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1));
+        mkey[lane] = ok ? key : 0;
+        mout[lane] = a.out + (ok ? k : 0) * (int64_t)v;
+        __syncwarp();
+        const int ng = (rows + G - 1) / G;
+        auto issue = [&](int g) {
+            U *buf = bufs + (g & 1) * G * sw;
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const int r = g * G + q;
+                if (r < rows && ((okm >> r) & 1) && lane < nq16)
+                    cp_async16(buf + q * sw + lane * per16, a.s.comp + mkey[r] * v + lane * per16);
+            }
+            cp_async_commit();
+        };
+        issue(0);
+        for (int g = 0; g < ng; ++g) {
+            if (g + 1 < ng) {
+                issue(g + 1);
+                cp_async_wait_one();
+            } else {
+                cp_async_wait_all();
+            }
+            __syncwarp();
+            hbm_decode_group<U, NC, G>(bufs + (g & 1) * G * sw, sw, g * G, rows, okm, pm, v, mw,
+                                       lt, mout, a.status);
+            __syncwarp();
+        }
+    }
+}
+
+// Device rows of at most 64 words, each 16-byte aligned, fetched whole by hbm_rows_kernel
+// (not the sorted mode, whose positions repeat keys, nor raw gathers or condensed rows).
+template <typename U>
+static bool hbm_rows_fit(const FetchArgs<U> &a) {
+    return a.device_rows && !a.raw_only && !a.dedup && !a.pos && !a.s.offsets && a.s.v <= 64 &&
+           (a.s.v * (int64_t)sizeof(U)) % 16 == 0 && (((uintptr_t)a.s.comp) & 15) == 0;
+}
+
+template <typename U, int NC>
+static ibp_status launch_hbm_nc(FetchArgs<U> a, cudaStream_t st) {
+    constexpr int G = 8;
+    constexpr int threads = 256;
+    a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, 16 / sizeof(U));
+    const size_t smem = (size_t)(threads / 32) * (512 + 2 * G * a.slot_words * sizeof(U));
+    auto kern = hbm_rows_kernel<U, NC, G>;
+    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    if (per_sm < 1) per_sm = 1;
+    int64_t blocks = (int64_t)device_sm_count() * per_sm;
+    const int64_t need = (a.nrows + 32 * (threads / 32) - 1) / (32 * (threads / 32));
+    if (!a.list && blocks > need) blocks = need;
+    const int slot = profile_begin(st);
+    kern<<<(unsigned)blocks, threads, smem, st>>>(a);
+    IBP_LAUNCHED("hbm_rows_kernel");
+    profile_end(slot, st);
+    return IBP_OK;
 }
 
 // ------------------------------------------------------------------ repeats
@@ -446,7 +481,7 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     // row slots per warp: up to kRowsInFlight within ~96 KB per block; long rows get fewer
     // slots and then fewer warps
     // (plus 512 bytes per warp for the in-fetch claims' slots and positions)
-    const size_t warp_extra = a.hkeys ? 64 * sizeof(int64_t) : 0;
+    const size_t warp_extra = a.claims.keys ? 64 * sizeof(int64_t) : 0;
     auto smem_of = [&](int s, int t) { return (slot_bytes * s + warp_extra) * (t / 32); };
     int slots = kRowsInFlight;
     while (slots > 1 && smem_of(slots, threads) > 96 * 1024) --slots;
@@ -509,6 +544,8 @@ static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStre
     } else {
         a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, per16);
     }
+    if (hbm_rows_fit(a))
+        return a.s.v > 32 ? launch_hbm_nc<U, 2>(a, st) : launch_hbm_nc<U, 1>(a, st);
     if (a.async_rows && !a.raw_only) return launch_fetch_x<U, false, true>(a, nblks, nthreads, st);
     return launch_fetch_x<U, false, false>(a, nblks, nthreads, st);
 }
@@ -550,6 +587,7 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     // decoded a group at a time (256-byte rows: 75 -> 61 us for 100k rows; smaller rows
     // decode too quickly for the extra bookkeeping to pay)
     a.async_rows = on_device && v * (int64_t)sizeof(U) >= 256;
+    a.device_rows = on_device;
     a.s.comp = comp;
     a.s.n = n;
     a.s.v = v;
@@ -600,9 +638,7 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         } else {
             // host rows: claims and repeat copies happen inside the fetch, hidden behind its
             // PCIe reads
-            a.hkeys = hkeys;
-            a.hpos = hpos;
-            a.hslots = slots;
+            a.claims = ClaimTable{hkeys, hpos, slots, repeat_wait_polls()};
             return launch_fetch<U>(a, nblks, nthreads, st);
         }
         IBP_RET(launch_fetch<U>(a, nblks, nthreads, st));

@@ -630,6 +630,182 @@ __device__ __forceinline__ void fetch_heads_exact(const RowSet<U> &s, const Lane
     }
 }
 
+// ------------------------------------------------------------------ hashed dedup
+// The first position to claim a row in an open-addressing table fetches it; later ones are
+// repeats.  Tables have at least twice as many slots as positions, so linear probing ends
+// quickly.
+__device__ __forceinline__ uint64_t row_hash(int64_t key, int64_t slots) {
+    return __umul64hi((uint64_t)key * 0x9E3779B97F4A7C15ull, (uint64_t)slots);
+}
+
+// The table slot holding `key` after this call: claimed by it (`won`) or by an earlier one;
+// -1 when the table is full (it never is: it has twice as many slots as positions).
+__device__ __forceinline__ int64_t hash_claim_slot(int64_t *keys, int64_t slots, int64_t key,
+                                                   bool &won) {
+    won = false;
+    uint64_t h = row_hash(key, slots);
+    for (int64_t probe = 0; probe < slots; ++probe) {
+        // a plain read first: a row already claimed (hot rows of a skewed batch) costs no
+        // atomic, so repeats do not queue on one address
+        const int64_t cur = *reinterpret_cast<volatile int64_t *>(keys + h);
+        if (cur == key) return (int64_t)h;
+        if (cur == -1) {
+            const unsigned long long old = atomicCAS(
+                reinterpret_cast<unsigned long long *>(keys + h), ~0ull, (unsigned long long)key);
+            if (old == ~0ull) {
+                won = true;
+                return (int64_t)h;
+            }
+            if ((int64_t)old == key) return (int64_t)h;
+        }
+        h = h + 1 == (uint64_t)slots ? 0 : h + 1;
+    }
+    return -1;
+}
+
+__device__ __forceinline__ int64_t load_acquire(const int64_t *p) {
+    int64_t x;
+    asm volatile("ld.acquire.gpu.global.s64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
+    return x;
+}
+
+__device__ __forceinline__ void store_release(int64_t *p, int64_t x) {
+    asm volatile("st.release.gpu.global.s64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
+}
+
+// Copy rows src -> dst for the lanes of `dm` (each lane's src/dst), four rows at a time: all
+// four rows' loads before any store (16-byte moves when the rows are aligned), so the loads'
+// latencies overlap.  Sources are read through L2 (other SMs may have just written them).
+template <typename U>
+__device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_row, int64_t v,
+                                          bool vec_rows) {
+    constexpr int R = 4;
+    const int lane = threadIdx.x & 31;
+    while (dm) {
+        const U *src[R];
+        U *dst[R];
+        int cnt = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            src[r] = src_row;
+            dst[r] = dst_row;
+            if (dm) {
+                const int j = __ffs(dm) - 1;
+                dm &= dm - 1;
+                src[r] = reinterpret_cast<const U *>(__shfl_sync(
+                    0xffffffffu, reinterpret_cast<unsigned long long>(src_row), j));
+                dst[r] = reinterpret_cast<U *>(__shfl_sync(
+                    0xffffffffu, reinterpret_cast<unsigned long long>(dst_row), j));
+                cnt = r + 1;
+            }
+        }
+        if (vec_rows) {
+            const int64_t n16 = v * (int64_t)sizeof(U) / 16;
+            for (int64_t q = lane; q < n16; q += 32) {
+                uint4 t[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) t[r] = __ldcg(reinterpret_cast<const uint4 *>(src[r]) + q);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
+            }
+        } else {
+            for (int64_t q = lane; q < v; q += 32) {
+                U t[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) t[r] = __ldcg(src[r] + q);
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < cnt) dst[r][q] = t[r];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ in-fetch claims
+// A fetch kernel over host rows de-duplicates inside itself: each chunk of positions claims
+// its distinct rows in a hash table before fetching them (claim_chunk), and once the chunk's
+// claimed rows are written, publishes their output rows in the table and copies every repeat
+// from the output row of its row's first claim (settle_chunk), so the copies overlap the
+// other warps' host reads.  A warp waits only after publishing all of its own claims, so
+// every row waited on belongs to a warp that is still fetching and waits on nothing; the
+// wait is bounded all the same, and a repeat that stops waiting fetches its own row.
+constexpr int64_t kRowDone = 1ll << 62;  // a published table entry: output row address | this
+
+struct ClaimTable {
+    int64_t *keys;   // row keys (-1 = empty slot)
+    int64_t *rows;   // output row address of each slot's claim, | kRowDone once written (-1 before)
+    int64_t slots;
+    int wait_polls;  // polls (~0.25 us apart) a repeat makes for its row
+};
+
+// One claim per distinct key of the chunk (its lowest `head` lane).  On return `head` is set
+// for the lanes that fetch their row (they claimed it); the result is true for repeats
+// (their key was claimed by another lane or an earlier chunk).  Each lane parks its table slot
+// (| kRowDone when it claimed) and its output row address in `park` (64 words of shared
+// memory per warp) until the chunk is settled, which keeps them out of the fetch's registers.
+__device__ __forceinline__ bool claim_chunk(const ClaimTable &c, int64_t *park, int64_t key,
+                                            bool &head, const void *orow) {
+    const int lane = threadIdx.x & 31;
+    const unsigned same = __match_any_sync(0xffffffffu, head ? key : (int64_t)-1);
+    const int first = __ffs(same) - 1;
+    bool won = false;
+    int64_t slot = -1;
+    if (head && first == lane) slot = hash_claim_slot(c.keys, c.slots, key, won);
+    slot = __shfl_sync(0xffffffffu, slot, first);
+    const bool rep = head && !won && slot >= 0;
+    // a lane whose claim found the table full (a caller that understated the batch) fetches
+    // its row without a claim
+    head = won || (head && slot < 0);
+    park[lane] = won ? slot | kRowDone : (rep ? slot : -1);
+    park[32 + lane] = (int64_t)reinterpret_cast<uintptr_t>(orow);
+    return rep;
+}
+
+// After the chunk's claimed rows are written: publish them (every lane's stores are ordered
+// before the release by the warp barrier), then copy each repeat once its row is published.
+// Returns true for the repeats that gave up waiting (status bit 3); they fetch their own row.
+template <typename U>
+__device__ __forceinline__ bool settle_chunk(const ClaimTable &c, const int64_t *park, bool rep,
+                                             int64_t v, int32_t *status) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    const int64_t cw = park[lane];
+    U *const dst = reinterpret_cast<U *>(static_cast<uintptr_t>(park[32 + lane]));
+    const int64_t slot = cw & ~kRowDone;
+    if (cw >= 0 && (cw & kRowDone))
+        store_release(c.rows + slot, (int64_t)reinterpret_cast<uintptr_t>(dst) | kRowDone);
+    if (!__any_sync(0xffffffffu, rep)) return false;
+    // once any wait has given up, later ones make a single check (lane 0 reads the status
+    // word, so that every lane has the same bound)
+    int limit = 0;
+    if (lane == 0)
+        limit = (*reinterpret_cast<volatile int32_t *>(status) & kStatusWaitTimeout)
+                    ? min(1, c.wait_polls)
+                    : c.wait_polls;
+    limit = __shfl_sync(0xffffffffu, limit, 0);
+    const U *src = nullptr;
+    for (int it = 0; it < limit; ++it) {
+        if (rep && !src) {
+            const int64_t hv = load_acquire(c.rows + slot);
+            if (hv >= 0 && (hv & kRowDone))
+                src = reinterpret_cast<const U *>(static_cast<uintptr_t>(hv & ~kRowDone));
+        }
+        if (__all_sync(0xffffffffu, !rep || src)) break;
+        if (it + 1 < limit) __nanosleep(256);
+    }
+    const bool go = rep && src;
+    const bool vec = ((v * (int64_t)sizeof(U)) & 15) == 0 &&
+                     __all_sync(0xffffffffu, !go || (((reinterpret_cast<uintptr_t>(src) |
+                                                        reinterpret_cast<uintptr_t>(dst)) & 15) == 0));
+    copy_rows<U>(__ballot_sync(0xffffffffu, go), go ? src : dst, dst, v, vec);
+    const bool lost = rep && !src;
+    if (lost) atomicOr(status, kStatusWaitTimeout);
+    return lost;
+}
+
 // ------------------------------------------------------------------ repeats
 // First position of `target` in the sorted keys[0..hi] (keys[hi] == target): a 32-way
 // search, one probe per lane per round.

@@ -7,30 +7,66 @@
 // synchronisation a cudaMalloc/cudaFree can cause.  ibp_decompress_fetch_noalloc serves them
 // from a scratch array that this library reserves statically in device memory.
 //
-// The scratch is the file-scope array below (kNoAllocScratchBytes, 4 MiB); every device that
-// loads the library keeps it until the process exits.  Host code must not pass the array's
-// name to a kernel (on the host it names a host-side stand-in, not device memory): the first
-// call on each device looks up the array's device address with cudaGetSymbolAddress, with
-// that device current, and caches it.  That first call should therefore come before any
-// stream capture on that device.  All calls share the one array, which keeps whatever the
-// last call left in it; the fetch path rewrites every byte it reads (status word, column
-// tables, sort buffers) before use, so nothing is carried over between calls.  Calls whose
-// GPU work overlaps -- on different streams or from different threads -- race on the array
-// and must be serialised by the caller.
+// The scratch is the file-scope array below (IBP_NOALLOC_SCRATCH_BYTES, 4 MiB); every device
+// that loads the library keeps it until the process exits.  Host code must not pass the
+// array's name to a kernel (on the host it names a host-side stand-in, not device memory):
+// the first call in each CUDA context looks up the array's device address with
+// cudaGetSymbolAddress, with that context's device current, and caches it with the context's
+// unique id; a later call in another context of the device (after cudaDeviceReset, say, when
+// the module is loaded again and the array may move) looks it up again.  That first call
+// should therefore come before any stream capture on that device.  All calls share the one
+// array, which keeps whatever the last call left in it; the fetch path rewrites every byte it
+// reads (status word, column tables, sort buffers) before use, so nothing is carried over
+// between calls.  Calls whose GPU work overlaps -- on different streams or from different
+// threads -- race on the array and must be serialised by the caller.  The status word of the
+// last call is the array's first 4 bytes (ibp_decompress_fetch_noalloc_status).
+#include <cuda.h>  // driver types for cuCtxGetCurrent / cuCtxGetId (no libcuda link)
+
 #include <mutex>
 
 #include "ibp_internal.cuh"
 
 namespace ibp200 {
 
-constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;
+constexpr size_t kNoAllocScratchBytes = IBP_NOALLOC_SCRATCH_BYTES;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
+// Unique id of the calling thread's current CUDA context (0 when none is current or the
+// driver does not provide the query).  Ids are never reused within a process, so a cached
+// address tagged with one cannot outlive its context unnoticed.
+static unsigned long long current_context_id() {
+    typedef CUresult (*GetCurrent)(CUcontext *);
+    typedef CUresult (*GetId)(CUcontext, unsigned long long *);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void **)&get_current, cudaEnableDefault,
+                                    &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", (void **)&get_id, cudaEnableDefault, &q) !=
+                cudaSuccess || q != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+        cudaGetLastError();
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the static scratch in the current device's context.
 static ibp_status noalloc_scratch(void **out) {
     constexpr int kMaxDevices = 64;
+    struct Entry {
+        unsigned long long ctx;
+        void *addr;
+    };
     static std::mutex mu;
-    static void *addr[kMaxDevices] = {};
+    static Entry cache[kMaxDevices] = {};
     int dev = 0;
     IBP_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) {
@@ -39,17 +75,20 @@ static ibp_status noalloc_scratch(void **out) {
         return IBP_ERR_UNSUPPORTED;
     }
     std::lock_guard<std::mutex> g(mu);
-    if (!addr[dev]) {
+    const unsigned long long ctx = current_context_id();
+    if (!cache[dev].addr || ctx == 0 || ctx != cache[dev].ctx) {
         void *p = nullptr;
+        // also makes the device's primary context current on this thread if it was not
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
             set_error("decompress_fetch_noalloc: cudaGetSymbolAddress of the static scratch "
                       "failed: %s", cudaGetErrorString(e));
             return IBP_ERR_CUDA;
         }
-        addr[dev] = p;
+        cache[dev].addr = p;
+        cache[dev].ctx = current_context_id();  // 0 (no id available): look up every call
     }
-    *out = addr[dev];
+    *out = cache[dev].addr;
     return IBP_OK;
 }
 
@@ -87,6 +126,14 @@ ibp_status ibp_decompress_fetch_noalloc(const void *comp, int64_t num_vecs, int6
     return ibp_decompress_fetch(comp, num_vecs, vec_size, word_bytes, mask, bitval, bitmask, index,
                                 num_index, comp_len, out, -1, -1, -1, scratch,
                                 kNoAllocScratchBytes, stream);
+}
+
+ibp_status ibp_decompress_fetch_noalloc_status(int32_t *status, ibp_stream_t stream) {
+    clear_error();
+    IBP_ARG(status, "decompress_fetch_noalloc_status: null pointer");
+    void *scratch = nullptr;
+    IBP_RET(noalloc_scratch(&scratch));
+    return ibp_read_status(scratch, status, stream);
 }
 
 }  // extern "C"

@@ -2,8 +2,10 @@
 //
 // Clients submit requests (registered set, host row list, count) from any thread; a
 // scheduler thread admits them in arrival order as output memory frees up, packs every
-// admitted request into one batched launch (ibp_batch_fetch_sorted over the set registry:
-// every request's rows sorted and de-duplicated on the device), and
+// admitted request into one batched launch (ibp_batch_fetch_hashed over the set registry:
+// every (set, row) of the batch claimed in a hash table inside the fetch, so each crosses
+// the bus once and its repeats are copied on the device; ibp_server_set_dedup picks the
+// radix-sorted batch, ibp_batch_fetch_sorted, instead), and
 // keeps up to `max_inflight` batches on the GPU at once, so requests that arrive while
 // others run join the next launch instead of waiting for the queue to drain.  Completion is
 // stamped by a thread that waits on each batch's event in launch order.
@@ -14,7 +16,8 @@
 //   * index staging: a pinned host ring and a device ring of the same size; submit copies the
 //     client's row list into the host ring, the batch copies its span to the device ring;
 //   * request tables: one pinned + one device table per in-flight batch;
-//   * one sort workspace for max(index capacity, 2^20) rows (batches run in stream order).
+//   * one batch workspace (claim table or sort buffers) for max(index capacity, 2^20) rows
+//     (batches run in stream order).
 //
 // The reference has no serving layer: its callers (ColossalAI embedding bags, FlexGen
 // layers, DGL samplers) call decompress_fetch once per lookup.
@@ -82,6 +85,7 @@ struct Server {
     void *ws = nullptr;
     size_t ws_bytes = 0;
     int64_t sort_cap = 0;  // rows a de-duplicating batch may hold (workspace size)
+    int dedup = 0;         // 0: hashed batches, 1: sorted batches
     int64_t batch_rows = 0, batch_bytes = 0;  // admission limits of one batch
     cudaStream_t stream = nullptr;
     int device = 0;
@@ -274,15 +278,19 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
     }
     cudaMemcpyAsync(td, th, kTableHeader + sizeof(ibp_request) * recs.size(),
                     cudaMemcpyHostToDevice, s->stream);
-    // a batch that fits the sort workspace is de-duplicated and fetched in row order; a
-    // single range request beyond it (already in row order, no repeats) goes unsorted
+    // a batch that fits the workspace is de-duplicated (hash claims inside the fetch, or a
+    // radix sort); a single range request beyond it (distinct rows in order) goes as listed
     const ibp_request *dreq = reinterpret_cast<const ibp_request *>(td + kTableHeader);
-    ibp_status st =
-        rows <= s->sort_cap
-            ? ibp_batch_fetch_sorted(s->registry, dreq, (int32_t)recs.size(), rows, s->ws,
-                                     s->ws_bytes, s->stream)
-            : ibp_batch_fetch(s->registry, dreq, reinterpret_cast<const int32_t *>(td),
-                              s->max_batch, s->ws, s->ws_bytes, s->stream);
+    ibp_status st;
+    if (rows > s->sort_cap)
+        st = ibp_batch_fetch(s->registry, dreq, reinterpret_cast<const int32_t *>(td),
+                             s->max_batch, s->ws, s->ws_bytes, s->stream);
+    else if (s->dedup == 1)
+        st = ibp_batch_fetch_sorted(s->registry, dreq, (int32_t)recs.size(), rows, s->ws,
+                                    s->ws_bytes, s->stream);
+    else
+        st = ibp_batch_fetch_hashed(s->registry, dreq, (int32_t)recs.size(), rows, s->ws,
+                                    s->ws_bytes, s->stream);
     cudaEventRecord(s->tbl_event[table], s->stream);
     lk.lock();
     if (st != IBP_OK) s->err = ibp_last_error();
@@ -372,7 +380,8 @@ ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int
     s->sort_cap = std::min<int64_t>(std::max<int64_t>(index_capacity, 1 << 20), INT32_MAX);
     s->batch_rows = s->sort_cap;
     s->batch_bytes = kDefaultBatchBytes;
-    s->ws_bytes = std::max<size_t>(ibp_batch_fetch_sorted_workspace_size(s->sort_cap, max_batch),
+    s->ws_bytes = std::max<size_t>(std::max(ibp_batch_fetch_sorted_workspace_size(s->sort_cap, max_batch),
+                                            ibp_batch_fetch_hashed_workspace_size(s->sort_cap)),
                                    ibp_batch_fetch_workspace_size());
     if ((e = cudaMalloc(&s->ws, s->ws_bytes)) != cudaSuccess) return fail(e, "workspace");
     s->thr = std::thread(scheduler, s);
@@ -513,6 +522,16 @@ ibp_status ibp_server_set_batch_limits(ibp_server *srv, int64_t max_rows, int64_
     std::lock_guard<std::mutex> g(s->mu);
     if (max_rows > 0) s->batch_rows = std::min(max_rows, s->sort_cap);
     if (max_bytes > 0) s->batch_bytes = max_bytes;
+    return IBP_OK;
+}
+
+ibp_status ibp_server_set_dedup(ibp_server *srv, int32_t mode) {
+    clear_error();
+    Server *s = reinterpret_cast<Server *>(srv);
+    IBP_ARG(s, "server_set_dedup: null server");
+    IBP_ARG(mode == 0 || mode == 1, "server_set_dedup: mode must be 0 (hash) or 1 (sort)");
+    std::lock_guard<std::mutex> g(s->mu);
+    s->dedup = mode;
     return IBP_OK;
 }
 

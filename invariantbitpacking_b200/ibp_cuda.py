@@ -247,10 +247,36 @@ def compress_condensed(dataset, mask, bitval, index_array_=None):
     return comp, offs
 
 
+def _raise_on_status(ws, what):
+    """check=True: read the call's device status word (blocking) and raise for the rows the
+    call could not produce (an out-of-range index, a row whose bitmap does not fit its
+    mask); bit 3 (a repeat decoded its own row after waiting) leaves the output correct."""
+    if ws is None:
+        return
+    import ctypes
+    st = torch.zeros(1, dtype=torch.int32)
+    _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), _stream()))
+    bits = int(st[0])
+    problems = []
+    if bits & 1:
+        problems.append("an index was out of range (its output rows were not written)")
+    if bits & 2:
+        problems.append("a row marked compressed has a bitmap that does not fit the mask "
+                        "(the bitmask/mask do not belong to the data; its output row was not "
+                        "written)")
+    if problems:
+        raise RuntimeError(f"{what}: " + "; ".join(problems))
+
+
 def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=None,
                      index_array_=None, nblks_=None, nthreads_=None, impl_=None,
-                     output_tensor=None):
-    """src/decompress.cu:10-156 -> decompressed rows (non-blocking)."""
+                     output_tensor=None, *, check=False):
+    """src/decompress.cu:10-156 -> decompressed rows (non-blocking).
+
+    check=True (keyword only; no counterpart in the reference) waits for the call and raises
+    RuntimeError when an index was out of range or a row could not be decoded; the default
+    leaves those rows unwritten without a host synchronisation (print_debug(True) prints a
+    message instead)."""
     _torch_check(comp_dataset.device.type == "cuda" or comp_dataset.is_pinned(),
                  "Input tensor must accessible by CUDA device (GPU or pinned memory)")
     _torch_check(comp_dataset.dim() in (1, 2),
@@ -306,7 +332,9 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
             -1 if idx is None else nrows, comp_len, _ptr(out),
             -1 if nblks_ is None else int(nblks_),
             -1 if nthreads_ is None else int(nthreads_), impl, _ptr(ws), wsb, _stream()))
-        if _debug and ws is not None:
+        if check:
+            _raise_on_status(ws, "decompress_fetch")
+        elif _debug and ws is not None:
             st = torch.zeros(1, dtype=torch.int32)
             import ctypes
             _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), _stream()))
@@ -316,13 +344,14 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
 
 
 def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, out_device,
-                               index_array_=None, output_tensor=None):
+                               index_array_=None, output_tensor=None, *, check=False):
     """Rows of the condensed layout written by compress_condensed (no reference
     counterpart: the reference writes this layout but cannot read it back on the GPU).
 
     comp: the condensed words (1-D, device or pinned host); offsets: the inclusive byte
     offsets compress_condensed returned (int64, one per row; device, or pinned host).
-    Returns [len(index) or num_rows, vec_size] decompressed rows (non-blocking)."""
+    Returns [len(index) or num_rows, vec_size] decompressed rows (non-blocking; check=True
+    waits and raises for out-of-range indices and rows that cannot be decoded)."""
     _torch_check(comp.device.type == "cuda" or comp.is_pinned(),
                  "Input tensor must accessible by CUDA device (GPU or pinned memory)")
     _torch_check(comp.is_contiguous(), "Input tensor must be contiguous")
@@ -373,7 +402,9 @@ def decompress_fetch_condensed(comp, offsets, mask, bitval, vec_size, out_device
         _check(_lib.ibp_decompress_fetch_condensed(
             _ptr(comp), comp.numel(), _ptr(offsets), n, v, wb, _ptr(mask), _ptr(bitval), _ptr(idx),
             -1 if idx is None else nrows, _ptr(out), _ptr(ws), wsb, _stream()))
-        if _debug and ws is not None:
+        if check:
+            _raise_on_status(ws, "decompress_fetch_condensed")
+        elif _debug and ws is not None:
             st = torch.zeros(1, dtype=torch.int32)
             import ctypes
             _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), _stream()))

@@ -8,8 +8,9 @@
     srv.release(rid)                # rows go back to the arena
 
 Requests are admitted in arrival order as their output fits the arena and join the next
-batched launch (de-duplicated, up to the batch limits: 128 MiB of output by default), with
-up to `max_inflight` launches on the GPU.
+batched launch (de-duplicated by hash claims inside the fetch, or by a sort after
+set_dedup("sort"); up to the batch limits: 128 MiB of output by default), with up to
+`max_inflight` launches on the GPU.
 """
 import ctypes
 
@@ -34,6 +35,14 @@ class Server:
         self.counts = {}
         if batch_bytes is not None or batch_rows is not None:
             self.set_batch_limits(batch_rows, batch_bytes)
+
+    def set_dedup(self, mode):
+        """How later batches find repeated rows: "hash" (claims inside the fetch; default) or
+        "sort" (a radix sort of the batch's rows first)."""
+        m = {"hash": 0, "sort": 1}.get(mode)
+        if m is None:
+            raise ValueError(f"set_dedup: mode must be 'hash' or 'sort', got {mode!r}")
+        _capi.check(_lib.ibp_server_set_dedup(self.handle, m))
 
     def set_batch_limits(self, rows=None, nbytes=None):
         """Cap one batch at `rows` rows and `nbytes` output bytes (None: keep)."""

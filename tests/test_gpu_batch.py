@@ -200,3 +200,87 @@ def test_batch_sorted_total_mismatch_is_flagged(ibp, sets):
         _capi.check(lib.ibp_batch_fetch_sorted(reg.buf.data_ptr(), dreq.data_ptr(), 1, 100,
                                                ws.data_ptr(), 16,
                                                torch.cuda.current_stream().cuda_stream))
+
+
+def test_batch_hashed_dedup_matches_sources(ibp, sets):
+    """Hash-claimed batches (ibp_batch_fetch_hashed): rows repeated within and across requests
+    of one set are fetched once and copied; every output row matches the source, and the
+    listed-order path agrees."""
+    from invariantbitpacking_b200.batch import BatchFetcher, SetRegistry
+    reg = SetRegistry([s[1] for s in sets])
+    bf = BatchFetcher(reg, max_requests=64)
+    rng = np.random.default_rng(12)
+    for k in (1, 7, 40, 64):
+        reqs = dup_requests(rng, sets, k)
+        outs = bf.fetch(reqs, dedup="hash")
+        check(outs, reqs, sets)
+        assert bf.status() == 0
+    reqs = dup_requests(rng, sets, 30)
+    # the same rows in two requests of one set share their claims
+    reqs.append((reqs[0][0],) + reqs[0][1:])
+    a = bf.fetch(reqs, dedup="hash")
+    torch.cuda.synchronize()
+    b = bf.fetch(reqs)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+
+
+def test_batch_hashed_bad_rows_and_waits(ibp, sets):
+    """Bad rows and set ids are flagged and skipped; with the repeat wait limit at 0 every
+    repeat decodes its own row (status bit 3) and the rows are still exact."""
+    from invariantbitpacking_b200.batch import BatchFetcher, SetRegistry
+    reg = SetRegistry([s[1] for s in sets[:2]])
+    bf = BatchFetcher(reg, max_requests=8)
+    good = torch.tensor([2, 0, 2, 1, 0], dtype=torch.int64, device="cuda")
+    bad = torch.tensor([1, 10 ** 9, -5, 1, 10 ** 9], dtype=torch.int64, device="cuda")
+    o2 = torch.zeros((2, 32), dtype=torch.int64, device="cuda")
+    reqs = [(0, good, 0, 5), (1, bad, 0, 5), (7, None, 0, 2), (1, None, 0, 0)]
+    outs = bf.outputs_for([reqs[0], reqs[1]]) + [o2] + bf.outputs_for([reqs[3]])
+    outs = bf.fetch(reqs, outs, dedup="hash")
+    torch.cuda.synchronize()
+    assert bf.status() & 1
+    assert np.array_equal(outs[0].cpu().numpy(), sets[0][0][[2, 0, 2, 1, 0]])
+    o = outs[1].cpu().numpy()
+    assert np.array_equal(o[0], sets[1][0][1]) and np.array_equal(o[3], sets[1][0][1])
+    assert outs[3].shape[0] == 0 and not o2.any()
+    ibp.set_repeat_wait_limit(0)
+    try:
+        rng = np.random.default_rng(13)
+        reqs = dup_requests(rng, sets[:2], 8)
+        outs = bf.fetch(reqs, dedup="hash")
+        check(outs, reqs, sets)
+        assert bf.status() == 8
+    finally:
+        ibp.set_repeat_wait_limit(None)
+
+
+def test_batch_hashed_understated_total(ibp, sets):
+    """A stated total below the requests' rows sets status bit 2; the claim table is then
+    undersized, and rows whose claim finds it full are fetched without one: every row is
+    still written."""
+    from invariantbitpacking_b200 import _capi
+    from invariantbitpacking_b200.batch import SetRegistry
+    reg = SetRegistry([s[1] for s in sets[:1]])
+    idx = torch.arange(0, 600, 3, dtype=torch.int64, device="cuda")
+    out = torch.zeros((200, 32), dtype=torch.int64, device="cuda")
+    rec = (_capi.Request * 1)()
+    rec[0].set, rec[0].index, rec[0].first, rec[0].count, rec[0].out = 0, idx.data_ptr(), 0, 200, out.data_ptr()
+    dreq = torch.frombuffer(bytearray(bytes(rec)), dtype=torch.uint8).cuda()
+    lib = _capi.lib
+    want = sets[0][0][idx.cpu().numpy()]
+    for total in (10, 150, 200):
+        ws = torch.empty(lib.ibp_batch_fetch_hashed_workspace_size(total), dtype=torch.uint8,
+                         device="cuda")
+        out.zero_()
+        _capi.check(lib.ibp_batch_fetch_hashed(reg.buf.data_ptr(), dreq.data_ptr(), 1, total,
+                                               ws.data_ptr(), ws.numel(),
+                                               torch.cuda.current_stream().cuda_stream))
+        torch.cuda.synchronize()
+        st = int(ws[:4].view(torch.int32).item())
+        assert (st & 4) == (4 if total != 200 else 0)
+        assert np.array_equal(out.cpu().numpy(), want)
+    with pytest.raises(_capi.IBPError):
+        _capi.check(lib.ibp_batch_fetch_hashed(reg.buf.data_ptr(), dreq.data_ptr(), 1, 100,
+                                               ws.data_ptr(), 16,
+                                               torch.cuda.current_stream().cuda_stream))

@@ -136,3 +136,75 @@ def test_in_fetch_repeats(ibp, oracle, pattern, aligned, where, layout):
     assert status.value == 0
     want = oracle.decompress(comp, m.cpu().numpy(), b.cpu().numpy(), bm.cpu().numpy(), idx)
     assert np.array_equal(out.view(nidx, v).cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("pattern", ["zipf", "one_row"])
+@pytest.mark.parametrize("layout", ["fixed", "condensed"])
+def test_repeat_wait_gives_up_and_decodes_from_source(ibp, oracle, pattern, layout):
+    """A repeat of a hashed host-row fetch whose first occurrence is not published within the
+    wait limit decodes its own row from the source.  With the limit at 0 polls every repeat
+    takes that path: status bit 3 reports it, and every output row is still the oracle's (a
+    bounded device wait made to run out; nothing faults)."""
+    import ctypes
+    from invariantbitpacking_b200 import _capi
+    lib = _capi.lib
+    rng = np.random.default_rng(78)
+    n, v = 30000, 64
+    d = make(rng, n, v, 8)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    if layout == "condensed":
+        ccomp, offs = ibp.compress_condensed(x, m, b)
+        offs = offs.cuda()
+    bm = ibp.compress_inplace(x, m, b)
+    cl = ibp.get_single_compress_len(x, m, b)
+    torch.cuda.synchronize()
+    comp = x.numpy().copy()
+    if pattern == "zipf":
+        idx = np.minimum(rng.zipf(1.1, 120000) - 1, n - 1).astype(np.int64)
+    else:
+        idx = np.full(20000, 4321, dtype=np.int64)
+    ti = torch.from_numpy(idx).cuda()
+    nidx = idx.size
+    out = torch.full((nidx, v), 7, dtype=torch.int64, device="cuda")
+    wsb = lib.ibp_decompress_fetch_workspace_size(nidx, v, 8, 1)
+    ws = torch.empty(wsb, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    status = ctypes.c_int32(-1)
+    _capi.check(lib.ibp_set_fetch_dedup(2))
+    _capi.check(lib.ibp_set_repeat_wait_limit(0))
+    try:
+        if layout == "fixed":
+            _capi.check(lib.ibp_decompress_fetch(
+                x.data_ptr(), n, v, 8, m.data_ptr(), b.data_ptr(), bm.data_ptr(), ti.data_ptr(),
+                nidx, cl, out.data_ptr(), -1, -1, -1, ws.data_ptr(), wsb, st))
+        else:
+            _capi.check(lib.ibp_decompress_fetch_condensed(
+                ccomp.data_ptr(), ccomp.numel(), offs.data_ptr(), n, v, 8, m.data_ptr(),
+                b.data_ptr(), ti.data_ptr(), nidx, out.data_ptr(), ws.data_ptr(), wsb, st))
+        _capi.check(lib.ibp_read_status(ws.data_ptr(), ctypes.byref(status), st))
+    finally:
+        _capi.check(lib.ibp_set_repeat_wait_limit(-1))
+        _capi.check(lib.ibp_set_fetch_dedup(0))
+    assert status.value == 8  # bit 3 only: repeats gave up, nothing else went wrong
+    want = oracle.decompress(comp, m.cpu().numpy(), b.cpu().numpy(), bm.cpu().numpy(), idx)
+    assert np.array_equal(out.cpu().numpy(), want)
+
+
+def test_check_raises_for_out_of_range_index(ibp):
+    """check=True turns the status word into an error; the default stays non-blocking and
+    leaves the bad rows unwritten."""
+    rng = np.random.default_rng(79)
+    n, v = 5000, 64
+    d = make(rng, n, v, 8)
+    x = torch.from_numpy(d.copy()).pin_memory()
+    m, b = ibp.preprocess(x, None)
+    bm = ibp.compress_inplace(x, m, b)
+    good = torch.from_numpy(rng.integers(0, n, 700)).cuda()
+    out = ibp.decompress_fetch(x, m, b, bm, "cuda", None, good, check=True)
+    assert np.array_equal(out.cpu().numpy(), d[good.cpu().numpy()])
+    bad = torch.cat([good, torch.tensor([n], device="cuda")])
+    with pytest.raises(RuntimeError, match="out of range"):
+        ibp.decompress_fetch(x, m, b, bm, "cuda", None, bad, check=True)
+    out = ibp.decompress_fetch(x, m, b, bm, "cuda", None, bad)
+    assert np.array_equal(out[:-1].cpu().numpy(), d[good.cpu().numpy()])

@@ -274,3 +274,86 @@ def test_device_rows_whole_set_and_small_batches(ibp, oracle, wb, v):
         idx = rng.integers(0, n, k)
         out = ibp.decompress_fetch(xd, m, b, bm, "cuda", cl, torch.from_numpy(idx).cuda())
         assert np.array_equal(out.cpu().numpy(), d[idx])
+
+
+@pytest.mark.parametrize("wb,v", [(8, 2), (8, 16), (8, 48), (8, 64), (4, 4), (4, 32), (4, 64)])
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["auto", "sort", "hash"])
+def test_device_rows_up_to_64_words(ibp, oracle, wb, v, mode):
+    """Device rows of at most 64 words, 16-byte aligned (the whole-row HBM decode kernel for
+    unindexed and hash-listed fetches; the sort mode keeps the general kernel): raw and
+    compressed rows mixed, whole sets and batches with repeats, all exact."""
+    from invariantbitpacking_b200 import _capi
+    rng = np.random.default_rng(1000 + 10 * v + wb)
+    n = 3000
+    d, m, b = masked_rows(rng, n, v, wb, frac=0.7, flip=0.15)
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    x = torch.from_numpy(d.copy()).pin_memory()
+    bm = ibp.compress_inplace(x, dm, db)
+    xd = x.cuda()
+    _capi.check(_capi.lib.ibp_set_fetch_dedup(mode))
+    try:
+        out = ibp.decompress_fetch(xd, dm, db, bm, "cuda", None, None, check=True)
+        assert same(npy(out), d)
+        for k in (1, 31, 33, 700, 9000):
+            idx = rng.integers(0, n, k).astype(np.int64)
+            out = ibp.decompress_fetch(xd, dm, db, bm, "cuda", None, torch.from_numpy(idx).cuda(),
+                                       check=True)
+            assert same(npy(out), d[idx])
+    finally:
+        _capi.check(_capi.lib.ibp_set_fetch_dedup(0))
+
+
+@pytest.mark.parametrize("where", ["host", "device"])
+@pytest.mark.parametrize("wb,v", [(8, 64), (4, 64), (8, 24), (8, 200)])
+def test_corrupt_rows_are_flagged_and_skipped(ibp, oracle, where, wb, v):
+    """Rows stored raw but marked compressed in a doctored bitmask: a row whose bitmap claims
+    a stream as long as the raw row is reported (status bit 1, check=True raises) and its
+    output row left untouched; a row whose bitmap happens to fit is decoded as the oracle
+    decodes it."""
+    rng = np.random.default_rng(2000 + v + wb)
+    n = 2000
+    W = 8 * wb
+    d, m, b = masked_rows(rng, n, v, wb, frac=0.8, flip=0.05)
+    mw = -(-(-(-v // 8)) // wb)
+    # a tenth of the rows random (stored raw); half of those with a zero first (bitmap) part,
+    # which, marked compressed, claims every word raw: a stream longer than the row
+    noisy = rng.choice(n, n // 10, replace=False)
+    d[noisy] = rng.integers(-(2 ** 62), 2 ** 62, (noisy.size, v)).astype(d.dtype)
+    d.view(np.uint32).reshape(n, -1)[noisy[: noisy.size // 2], : mw * wb // 4] = 0
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    x = torch.from_numpy(d.copy()).pin_memory()
+    bm = ibp.compress_inplace(x, dm, db)
+    comp = x.numpy().copy()
+    bits = npy(bm).view(np.uint32)
+    raw = np.array([not (bits[r // 32] >> (r % 32)) & 1 for r in range(n)])
+    assert raw.any() and not raw.all()
+    bad_bits = bits.copy()
+    for r in np.flatnonzero(raw):
+        bad_bits[r // 32] |= np.uint32(1) << np.uint32(r % 32)
+    bm2 = torch.from_numpy(bad_bits.view(np.int32)).cuda()
+    # which doctored rows claim a stream too long for the row
+    ut = {4: np.uint32, 8: np.uint64}[wb]
+    nb = np.array([W - bin(int(x)).count("1") for x in m.view(ut)])
+    units = comp.view(np.uint32).reshape(n, -1)
+    too_long = np.zeros(n, dtype=bool)
+    for r in np.flatnonzero(raw):
+        cj = np.array([(units[r, j // 32] >> (j % 32)) & 1 for j in range(v)], dtype=bool)
+        total = int(np.where(cj, nb, W).sum())
+        too_long[r] = mw + -(-total // W) >= v
+    assert too_long.any()
+    src = x.cuda() if where == "device" else x
+    for idx in (None, rng.integers(0, n, 1500).astype(np.int64)):
+        rows = np.arange(n) if idx is None else idx
+        out = torch.full((rows.size, v), 7, dtype=x.dtype, device="cuda")
+        ti = None if idx is None else torch.from_numpy(idx).cuda()
+        with pytest.raises(RuntimeError, match="bitmap"):
+            ibp.decompress_fetch(src, dm, db, bm2, "cuda", None, ti, output_tensor=out,
+                                 check=True)
+        out.fill_(7)
+        ibp.decompress_fetch(src, dm, db, bm2, "cuda", None, ti, output_tensor=out)
+        got = npy(out)
+        skip = too_long[rows]
+        assert (got[skip] == 7).all()
+        keep = ~skip
+        want = oracle.decompress(comp, m, b, bad_bits.view(np.int32), rows[keep])
+        assert same(got[keep], want.view(d.dtype))

@@ -19,8 +19,9 @@ def ibp():
     return m
 
 
+@pytest.mark.parametrize("dedup", ["hash", "sort"])
 @pytest.mark.parametrize("limits", [None, (2000, 256 << 10)])
-def test_server_results_equal_solo_fetches(ibp, limits):
+def test_server_results_equal_solo_fetches(ibp, limits, dedup):
     from invariantbitpacking_b200.batch import SetRegistry
     from invariantbitpacking_b200.serve import Server
     rng = np.random.default_rng(5)
@@ -37,6 +38,7 @@ def test_server_results_equal_solo_fetches(ibp, limits):
     reg = SetRegistry(sets)
     srv = Server(reg, arena_bytes=64 << 20, index_capacity=1 << 20, max_batch=16,
                  max_inflight=2)
+    srv.set_dedup(dedup)
     if limits:
         srv.set_batch_limits(*limits)
     reqs = []

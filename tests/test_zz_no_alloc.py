@@ -5,8 +5,11 @@ Called through the C ABI with plain pointers and checked, bit for bit, against t
 ibp_decompress_fetch (caller-provided scratch) on two calls in a row -- different index
 arrays, word sizes and row lengths, so whatever the first call leaves in the shared scratch
 must not leak into the second -- and against the source rows.  A call that needs more
-scratch than the static array holds is refused before anything runs.  This file is named so
-that pytest collects it last."""
+scratch than the static array holds is refused before anything runs, and the status word of
+a call (here: an out-of-range index) is readable through ibp_decompress_fetch_noalloc_status.
+This file is named so that pytest collects it last."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -102,3 +105,31 @@ def test_noalloc_refuses_calls_beyond_its_scratch(eng):
     assert b"static" in lib.ibp_last_error()
     torch.cuda.synchronize()
     assert bool((out == 5).all())
+
+
+def _status(capi):
+    st = ctypes.c_int32(-1)
+    capi.check(capi.lib.ibp_decompress_fetch_noalloc_status(
+        ctypes.byref(st), torch.cuda.current_stream().cuda_stream))
+    return st.value
+
+
+def test_noalloc_status_reports_out_of_range_index(eng):
+    ibp, capi = eng
+    from invariantbitpacking_b200 import synthetic
+    assert capi.NOALLOC_SCRATCH_BYTES == LIMIT
+    d = synthetic.graph_features(n=3000, seed=33)
+    x, m, b, bm = _compressed(ibp, d)
+    rows = np.array([5, 2999, 3000, -1, 7, 5], dtype=np.int64)
+    idx = torch.from_numpy(rows).cuda()
+    a = _noalloc(capi, x, m, b, bm, idx, 64, 8, len(rows))
+    assert _status(capi) & 1  # bit 0: an index was out of range
+    a = a.cpu().numpy()
+    ok = (rows >= 0) & (rows < 3000)
+    assert np.array_equal(a[ok], d[rows[ok]])
+    assert (a[~ok] == -7).all()  # rows of bad indices are left untouched
+    # the next call starts from a clear status word
+    good = torch.from_numpy(rows[ok]).cuda()
+    a = _noalloc(capi, x, m, b, bm, good, 64, 8, int(ok.sum()))
+    assert _status(capi) == 0
+    assert np.array_equal(a.cpu().numpy(), d[rows[ok]])
