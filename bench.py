@@ -86,6 +86,8 @@ def parse():
                              "device_graph_features"])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=300)
+    ap.add_argument("--served-reps", type=int, default=3,
+                    help="served_mix: rounds of each arm per rate (medians reported)")
     ap.add_argument("--shard", action="store_true",
                     help="graph_features under torchrun: split every batch across the ranks "
                          "(strong scaling) instead of one replica per rank")
@@ -1289,43 +1291,45 @@ def run_served(args):
         total_bytes = int(sum(c * srcs[s].shape[1] * 8 for s, c in zip(sids, counts)))
 
         # ---- served: a client thread submits on schedule, the main thread waits/releases
-        ids = [None] * nreq
-        base = time.monotonic() + 0.05
+        def served_run(check):
+            nonlocal checked
+            ids = [None] * nreq
+            base = time.monotonic() + 0.05
 
-        def client():
+            def client():
+                for j in range(nreq):
+                    t = base + arrive[j]
+                    while time.monotonic() < t:
+                        pass
+                    while True:
+                        try:
+                            ids[j] = srv.submit(int(sids[j]), rows[j])
+                            break
+                        except RuntimeError:
+                            time.sleep(0.0002)
+
+            th = threading.Thread(target=client)
+            th.start()
+            lat = []
+            t_last = 0.0
+            kept = {}
             for j in range(nreq):
-                t = base + arrive[j]
-                while time.monotonic() < t:
-                    pass
-                while True:
-                    try:
-                        ids[j] = srv.submit(int(sids[j]), rows[j])
-                        break
-                    except RuntimeError:
-                        time.sleep(0.0002)
-
-        th = threading.Thread(target=client)
-        th.start()
-        lat = []
-        t_last = 0.0
-        kept = {}
-        for j in range(nreq):
-            while ids[j] is None:
-                time.sleep(0.0001)
-            out, tm = srv.wait(ids[j], 600000)
-            if j % 37 == 0:
-                kept[j] = out.clone()  # checked after the run: no host work while timing
-            srv.release(ids[j])
-            lat.append(tm[2] / 1e6 - (base + arrive[j]))
-            t_last = max(t_last, tm[2] / 1e6)
-        th.join()
-        for j, out in kept.items():
-            assert np.array_equal(out.cpu().numpy(), srcs[sids[j]][rows[j]]), "served mismatch"
-            checked += 1
-        del kept
-        served = {"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
-                  "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
-                  "GBps": round(total_bytes / (t_last - base) / 1e9, 3)}
+                while ids[j] is None:
+                    time.sleep(0.0001)
+                out, tm = srv.wait(ids[j], 600000)
+                if check and j % 37 == 0:
+                    kept[j] = out.clone()  # checked after the run: no host work while timing
+                srv.release(ids[j])
+                lat.append(tm[2] / 1e6 - (base + arrive[j]))
+                t_last = max(t_last, tm[2] / 1e6)
+            th.join()
+            for j, out in kept.items():
+                assert np.array_equal(out.cpu().numpy(), srcs[sids[j]][rows[j]]), "served mismatch"
+                checked += 1
+            del kept
+            return {"p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                    "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                    "GBps": round(total_bytes / (t_last - base) / 1e9, 3)}
 
         # ---- per request: one plain decompress_fetch per request, in arrival order (ours,
         # and the reference's own when its build is present)
@@ -1367,15 +1371,28 @@ def run_served(args):
                     "GBps": round(total_bytes / (max(done_t) - base2) / 1e9, 3)}
 
         dev = torch.device("cuda")
-        plain = per_request(lambda x, m, b, bm, cl, idx:
-                            ibp.decompress_fetch(x, m, b, bm, dev, cl, idx))
-        entry = {"rate_per_s": rate, "requests": nreq,
-                 "output_GB": round(total_bytes / 1e9, 2), "served": served,
-                 "per_request": plain}
+        arms = {"served": lambda rep: served_run(rep == 0),
+                "per_request": lambda rep: per_request(
+                    lambda x, m, b, bm, cl, idx: ibp.decompress_fetch(x, m, b, bm, dev, cl, idx))}
         if ref is not None:
-            entry["per_request_reference"] = per_request(
+            arms["per_request_reference"] = lambda rep: per_request(
                 lambda x, m, b, bm, cl, idx:
                 ref.decompress_fetch(x, m, b, bm, dev, cl, idx, None, None, None, None))
+        # the arms take turns, `reps` rounds in a rotating order, so a drift of the shared
+        # box's host or link speed during the run falls on every arm alike; each metric is
+        # the median over the rounds
+        names = list(arms)
+        runs = {a: [] for a in names}
+        for rep in range(args.served_reps):
+            order = names[rep % len(names):] + names[:rep % len(names)]
+            for a in order:
+                runs[a].append(arms[a](rep))
+        entry = {"rate_per_s": rate, "requests": nreq,
+                 "output_GB": round(total_bytes / 1e9, 2), "rounds": args.served_reps}
+        for a in names:
+            entry[a] = {k: round(float(np.median([r[k] for r in runs[a]])), 3)
+                        for k in ("p50_ms", "p99_ms", "GBps")}
+            entry[a]["rounds_GBps"] = [r["GBps"] for r in runs[a]]
         results.append(entry)
     st = srv.stats()
     srv.close()
@@ -1592,6 +1609,33 @@ def main():
 
     pcie = measured_pcie_h2d(torch)
 
+    # ---- the ceiling of the fetch kernel's access pattern: the same distinct rows of every
+    # batch, in the order the hashed fetch reads them (first occurrence), read as the kernel's
+    # first read (the comp_len hint rounded up to 32-byte sectors) and not decoded
+    first_bytes = -(-comp_len * 8 // 32) * 32
+    heads_dev = []
+    for bt in batches:
+        _, first = np.unique(bt, return_index=True)
+        heads_dev.append(torch.from_numpy(bt[np.sort(first)].astype(np.int64)).cuda())
+    for k in range(len(batches)):
+        hd = heads_dev[k]
+        _capi.check(lib.ibp_read_rows_probe(x.data_ptr(), V * 8, hd.data_ptr(), hd.shape[0],
+                                            first_bytes, wsp.data_ptr(), wsb, stream.cuda_stream))
+    _capi.check(lib.ibp_profile_enable(len(batches)))
+    for k in range(len(batches)):
+        hd = heads_dev[k]
+        _capi.check(lib.ibp_read_rows_probe(x.data_ptr(), V * 8, hd.data_ptr(), hd.shape[0],
+                                            first_bytes, wsp.data_ptr(), wsb, stream.cuda_stream))
+    pms = kernel_ms(len(batches))
+    pat_gbs = sum(uniq_bytes) / sum(pms) / 1e6
+    pattern = {"achieved": round(pat_gbs, 3), "frac_of_copy": round(pat_gbs / pcie, 4),
+               "read_bytes_per_row": int(first_bytes),
+               "kernel_frac_of_pattern": None,
+               "what": "ibp_read_rows_probe: the distinct rows of each batch, in first-occurrence "
+                       "order, read as the fetch kernel's first read and not decoded; "
+                       "compressed bytes of those rows / probe CUDA-event time"}
+    del heads_dev
+
     # ---- the same fetches of the uncompressed set (impl 2: plain zero-copy gather, same sort
     # and repeat fill): what the batch costs without compression
     raw = torch.from_numpy(d).pin_memory()
@@ -1751,7 +1795,9 @@ def main():
                          "peak_source": "pinned host->device copy measured in this run "
                                         "(no PCIe figure in MEASURED_PEAKS.json)",
                          "achieved_counting_repeats": round(fetch_gbs_dups, 3),
-                         "kernel_ms_per_launch": round(sum(kms) / len(kms), 4)},
+                         "kernel_ms_per_launch": round(sum(kms) / len(kms), 4),
+                         "pattern_ceiling": dict(pattern, kernel_frac_of_pattern=round(
+                             fetch_gbs / pat_gbs, 4))},
             "roofline_hbm": hbm,
             "cpu_baseline": cpu,
             "cpu_baseline_uncompressed_gather": gather,

@@ -189,6 +189,17 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                 int32_t nthreads, int32_t impl, void *workspace,
                                 size_t workspace_bytes, ibp_stream_t stream);
 
+/* Measurement aid, no counterpart in the reference: reads the first read_bytes (1..1024,
+ * rounded up to 16-byte blocks) of each listed row -- row r at base + r * stride_bytes, rows
+ * 16-byte aligned -- the way the row-fetch kernel does (a warp keeps 4 rows in flight, the
+ * same grid shape) and decodes nothing.  Its time, taken with the profiling hooks, is the
+ * ceiling of the fetch kernel's access pattern on this link or memory.  Each row is read
+ * entirely inside [base + r * stride_bytes, + read_bytes rounded up to 16), so the caller
+ * must own those bytes.  Workspace: 256 bytes of device memory. */
+ibp_status ibp_read_rows_probe(const void *base, int64_t stride_bytes, const int64_t *rows,
+                               int64_t num_rows, int32_t read_bytes, void *workspace,
+                               size_t workspace_bytes, ibp_stream_t stream);
+
 /* ---------------------------------------------------------------- condensed fetch
  * No counterpart in the reference, which writes the condensed layout (compress_condensed,
  * src/compress.cu:238-313) but has no decompressor for it.  out row k = decompressed row
@@ -321,11 +332,15 @@ ibp_status ibp_server_wait(ibp_server *srv, int64_t id, int32_t timeout_ms, void
 ibp_status ibp_server_cancel(ibp_server *srv, int64_t id);
 /* Give a finished request's output rows back to the arena. */
 ibp_status ibp_server_release(ibp_server *srv, int64_t id);
-/* Admission limits of one batch: at most max_rows rows (no more than the sort workspace's
+/* Admission limits of one batch: at most max_rows rows (no more than the batch workspace's
  * max(index_capacity, 2^20)) and max_bytes output bytes, both counted after the batch's
  * first request, which is always admitted.  <= 0 keeps the current value.  Defaults: the
- * sort workspace's rows and 128 MiB.  Smaller batches finish early requests of a burst
- * sooner (lower p50); larger ones amortise per-launch cost. */
+ * workspace's rows and 128 MiB.  When requests queue up faster than the link drains them,
+ * the byte limit rises to the queued output bytes divided by max_inflight, so a backlog is
+ * served by fewer, larger launches (which also share the rows that queued requests of one
+ * set have in common).  Smaller batches finish early requests of a burst sooner (lower
+ * p50); larger ones amortise per-launch cost.  Index spans and request tables are copied to
+ * the device on a second stream, overlapping the previous batch's kernel. */
 ibp_status ibp_server_set_batch_limits(ibp_server *srv, int64_t max_rows, int64_t max_bytes);
 /* How later batches de-duplicate: 0 = hash claims inside the fetch (default), 1 = radix sort
  * (rows then fetched in row order). */

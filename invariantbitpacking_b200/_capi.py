@@ -53,6 +53,7 @@ SIGNATURES = {
     "ibp_batch_fetch_workspace_size": (_SZ, []),
     "ibp_batch_fetch": (_INT, [_P, _P, _P, _I32, _P, _SZ, _P]),
     "ibp_batch_autotune": (_INT, [_P, _P, _P, _I32, _P, _SZ, _P, _P]),
+    "ibp_read_rows_probe": (_INT, [_P, _I64, _P, _I64, _I32, _P, _SZ, _P]),
     "ibp_decompress_fetch_condensed": (_INT, [_P, _I64, _P, _I64, _I64, _INT, _P, _P, _P, _I64,
                                                _P, _P, _SZ, _P]),
     "ibp_batch_fetch_sorted_workspace_size": (_SZ, [_I64, _I32]),

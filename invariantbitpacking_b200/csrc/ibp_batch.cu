@@ -634,6 +634,16 @@ struct HashedArgs {
 
 constexpr int kSetKeyShift = 40;  // claim key: (set << 40) | row
 
+// The long-row decode path of the hashed batch as a called function rather than inlined
+// beside the register-table path, so the two do not add up their register needs.
+template <typename U>
+__device__ __noinline__ void fetch_long_rows(const RowSet<U> &s, U *slots, int nslots,
+                                             int64_t slot_words, int64_t key, U *orow,
+                                             bool head, bool packed, int32_t *status) {
+    LaneTables<U, 0> lt0;
+    fetch_heads<U, 0>(s, lt0, slots, nslots, slot_words, key, orow, head, packed, status);
+}
+
 template <typename U>
 __global__ void __launch_bounds__(256, 2) batch_fetch_hashed_kernel(HashedArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -652,7 +662,6 @@ __global__ void __launch_bounds__(256, 2) batch_fetch_hashed_kernel(HashedArgs<U
         if (rows != a.total) atomicOr(a.status, kStatusBadTable);
     }
     LaneTables<U, 2> lt;  // register tables of the current set when its rows are short
-    LaneTables<U, 0> lt0;
     int cur_set = -1;
     for (;;) {
         unsigned long long u = 0;
@@ -689,7 +698,7 @@ __global__ void __launch_bounds__(256, 2) batch_fetch_hashed_kernel(HashedArgs<U
             if (small)
                 fetch_heads<U, 2>(s, lt, slots, ns, sw, key, orow, fetch_lane, packed, a.status);
             else
-                fetch_heads<U, 0>(s, lt0, slots, ns, sw, key, orow, fetch_lane, packed, a.status);
+                fetch_long_rows<U>(s, slots, ns, sw, key, orow, fetch_lane, packed, a.status);
             if (pass > 0) break;
             fetch_lane = settle_chunk<U>(a.claims, park, rep, s.v, a.status);
             if (!__any_sync(0xffffffffu, fetch_lane)) break;

@@ -503,6 +503,20 @@ ibp_status ibp_decompress_fetch(const void *comp, int64_t num_vecs, int64_t vec_
                                      nthreads, impl, workspace, workspace_bytes, st);
 }
 
+ibp_status ibp_read_rows_probe(const void *base, int64_t stride_bytes, const int64_t *rows,
+                               int64_t num_rows, int32_t read_bytes, void *workspace,
+                               size_t workspace_bytes, ibp_stream_t stream) {
+    clear_error();
+    IBP_ARG(base && (rows || num_rows == 0), "read_rows_probe: null argument");
+    IBP_ARG(num_rows >= 0, "read_rows_probe: negative row count");
+    IBP_ARG(read_bytes > 0 && read_bytes <= 1024, "read_rows_probe: read_bytes must be 1..1024");
+    IBP_ARG(stride_bytes >= read_bytes && stride_bytes % 16 == 0 && ((uintptr_t)base & 15) == 0,
+            "read_rows_probe: rows must be 16-byte aligned and at least read_bytes apart");
+    IBP_ACCESSIBLE(rows, "read_rows_probe", "the row list");
+    return read_rows_probe(base, stride_bytes, rows, num_rows, read_bytes, workspace,
+                           workspace_bytes, (cudaStream_t)stream);
+}
+
 // ------------------------------------------------------------------ condensed fetch
 ibp_status ibp_decompress_fetch_condensed(const void *comp, int64_t comp_words,
                                           const int64_t *offsets, int64_t num_vecs,

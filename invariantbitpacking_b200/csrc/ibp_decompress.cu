@@ -250,6 +250,23 @@ __device__ __forceinline__ U stream_bits(const U *words, uint32_t s, int L) {
     return L == 0 ? (U)0 : (U)(win >> (W - L));
 }
 
+// The same read from 32-bit units of the MSB-first stream with two funnel shifts: stream unit
+// t is memory unit t ^ 1 for 64-bit words (the high half of a little-endian word comes
+// second) and unit t for 32-bit words.  Reads the same words as stream_bits.
+template <typename U>
+__device__ __forceinline__ U stream_bits_funnel(const U *words, uint32_t s, int L) {
+    const uint32_t *u = reinterpret_cast<const uint32_t *>(words);
+    const uint32_t t = s >> 5, r = s & 31;
+    if constexpr (sizeof(U) == 8) {
+        const uint32_t a = u[t ^ 1], b = u[(t + 1) ^ 1], c = u[(t + 2) ^ 1];
+        const uint64_t win = ((uint64_t)__funnelshift_l(b, a, r) << 32) | __funnelshift_l(c, b, r);
+        return L == 0 ? (U)0 : (U)(win >> (64 - L));
+    } else {
+        const uint32_t win = __funnelshift_l(u[t + 1], u[t], r);
+        return L == 0 ? (U)0 : (U)(win >> (32 - L));
+    }
+}
+
 template <typename U, int NC, int G>
 __device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int sw, int r0,
                                                  int rows, unsigned okm, unsigned pm, int v,
@@ -311,57 +328,78 @@ __device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int 
             if (j < v) {
                 const bool cj = (cjm >> (q * NC + c)) & 1u;
                 const int L = cj ? (int)lt.nb[c] : W;
-                const U y = stream_bits<U>(stream, (c ? t0 : 0u) + incl[q][c] - (uint32_t)L, L);
+                const U y =
+                    stream_bits_funnel<U>(stream, (c ? t0 : 0u) + incl[q][c] - (uint32_t)L, L);
                 o[j] = cj ? (U)(lt.bv[c] | scatter_regs<U>(y, (U)~lt.m[c], lt.mv[c])) : y;
             }
         }
     }
 }
 
+// Shared memory of hbm_rows_kernel per warp: keys, output rows and stored-compressed flags
+// of its (up to) 32 rows, then two buffers of G row slots.
+constexpr size_t kHbmWarpMetaBytes = 512 + 128;
+
 template <typename U, int NC, int G>
-__global__ void __launch_bounds__(256, 3) hbm_rows_kernel(FetchArgs<U> a) {
+__global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int per16 = 16 / sizeof(U);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int64_t *mkey = reinterpret_cast<int64_t *>(smem) + warp * 64;
+    unsigned char *meta = smem + warp * kHbmWarpMetaBytes;
+    int64_t *mkey = reinterpret_cast<int64_t *>(meta);
     U **mout = reinterpret_cast<U **>(mkey + 32);
+    int32_t *mpk = reinterpret_cast<int32_t *>(meta + 512);
     const int sw = (int)a.slot_words;
-    U *bufs = reinterpret_cast<U *>(smem + (blockDim.x >> 5) * 512) + (int64_t)warp * 2 * G * sw;
+    U *bufs = reinterpret_cast<U *>(smem + (blockDim.x >> 5) * kHbmWarpMetaBytes) +
+              (int64_t)warp * 2 * G * sw;
     LaneTables<U, NC> lt;
     lt.load(a.s.t, a.s.v);
     const int v = (int)a.s.v, mw = (int)a.s.mw;
     const int nq16 = v / per16;  // 16-byte blocks of a row (<= 32)
     const int64_t nrows = a.list ? (int64_t)*a.list_len : a.nrows;
+    // chunks of 32 rows (double-buffered groups) when every warp gets several of them;
+    // otherwise one group per chunk, so that the rows spread over all warps
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int chunk = nrows >= 4 * 32 * nwarps ? 32 : G;
+    const unsigned below = (1u << lane) - 1u;
     for (;;) {
         unsigned long long c0 = 0;
-        if (lane == 0) c0 = atomicAdd(a.work, 32ull);
+        if (lane == 0) c0 = atomicAdd(a.work, (unsigned long long)chunk);
         const int64_t p0 = (int64_t)__shfl_sync(0xffffffffu, c0, 0);
         if (p0 >= nrows) break;
-        const int rows = (int)min((int64_t)32, nrows - p0);
-        const bool valid = lane < rows;
+        const int avail = (int)min((int64_t)chunk, nrows - p0);
+        const bool valid = lane < avail;
         const int64_t k = valid ? (a.list ? a.list[p0 + lane] : p0 + lane) : 0;
         const int64_t key = valid ? (a.keys ? a.keys[k] : k) : 0;
         const bool bad = valid && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         const bool ok = valid && !bad;
-        const unsigned okm = __ballot_sync(0xffffffffu, ok);
-        const unsigned pm = __ballot_sync(
-            0xffffffffu, ok && ((__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1));
-        mkey[lane] = ok ? key : 0;
-        mout[lane] = a.out + (ok ? k : 0) * (int64_t)v;
+        // the chunk's rows, packed to the front of its metadata
+        const unsigned fm = __ballot_sync(0xffffffffu, ok);
+        const int rows = __popc(fm);
+        if (ok) {
+            const int slot = __popc(fm & below);
+            mkey[slot] = key;
+            mout[slot] = a.out + k * (int64_t)v;
+            mpk[slot] = (__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1;
+        }
         __syncwarp();
+        const unsigned okm = rows == 32 ? 0xffffffffu : ((1u << rows) - 1u);
+        const unsigned pm = __ballot_sync(0xffffffffu, lane < rows && mpk[lane]);
         const int ng = (rows + G - 1) / G;
+        // groups of G whole rows: the next group is copied into the other buffer while this
+        // one decodes
         auto issue = [&](int g) {
             U *buf = bufs + (g & 1) * G * sw;
 #pragma unroll
             for (int q = 0; q < G; ++q) {
                 const int r = g * G + q;
-                if (r < rows && ((okm >> r) & 1) && lane < nq16)
+                if (r < rows && lane < nq16)
                     cp_async16(buf + q * sw + lane * per16, a.s.comp + mkey[r] * v + lane * per16);
             }
             cp_async_commit();
         };
-        issue(0);
+        if (ng > 0) issue(0);
         for (int g = 0; g < ng; ++g) {
             if (g + 1 < ng) {
                 issue(g + 1);
@@ -381,23 +419,27 @@ __global__ void __launch_bounds__(256, 3) hbm_rows_kernel(FetchArgs<U> a) {
 // (not the sorted mode, whose positions repeat keys, nor raw gathers or condensed rows).
 template <typename U>
 static bool hbm_rows_fit(const FetchArgs<U> &a) {
-    return a.device_rows && !a.raw_only && !a.dedup && !a.pos && !a.s.offsets && a.s.v <= 64 &&
+    return a.device_rows && !a.raw_only && !a.dedup && !a.pos && !a.s.offsets &&
+           !a.claims.keys && a.s.v <= 64 &&
            (a.s.v * (int64_t)sizeof(U)) % 16 == 0 && (((uintptr_t)a.s.comp) & 15) == 0;
 }
 
 template <typename U, int NC>
 static ibp_status launch_hbm_nc(FetchArgs<U> a, cudaStream_t st) {
-    constexpr int G = 8;
+    // groups of 4 rows: measured faster than 8 (37 against 39 us for the 79k distinct rows of
+    // a 400k-row graph-feature batch), with half the shared memory
+    constexpr int G = 4;
     constexpr int threads = 256;
     a.slot_words = (int64_t)align_up((size_t)a.s.v + 2, 16 / sizeof(U));
-    const size_t smem = (size_t)(threads / 32) * (512 + 2 * G * a.slot_words * sizeof(U));
+    const size_t smem =
+        (size_t)(threads / 32) * (kHbmWarpMetaBytes + 2 * G * a.slot_words * sizeof(U));
     auto kern = hbm_rows_kernel<U, NC, G>;
     IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
     if (per_sm < 1) per_sm = 1;
     int64_t blocks = (int64_t)device_sm_count() * per_sm;
-    const int64_t need = (a.nrows + 32 * (threads / 32) - 1) / (32 * (threads / 32));
+    const int64_t need = (a.nrows + (int64_t)G * (threads / 32) - 1) / ((int64_t)G * (threads / 32));
     if (!a.list && blocks > need) blocks = need;
     const int slot = profile_begin(st);
     kern<<<(unsigned)blocks, threads, smem, st>>>(a);
@@ -670,6 +712,67 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     fill_repeats_kernel<U, CallRows<U>><<<(unsigned)fb, 256, 0, st>>>(keys, nidx,
                                                                        CallRows<U>{out, pos, v, n});
     IBP_LAUNCHED("fill_repeats_kernel");
+    return IBP_OK;
+}
+
+// ------------------------------------------------------------------ access-pattern probe
+// Reads the first `nq` 16-byte blocks of each listed row the way fetch_heads does (a warp
+// takes kRowsInFlight rows from a work counter, all their loads before any is consumed) and
+// decodes nothing, so its time is what the fetch kernel's reads alone cost on this link.
+__global__ void __launch_bounds__(kFetchThreads, 2)
+read_rows_probe_kernel(const uint4 *__restrict__ base, int64_t stride16,
+                       const int64_t *__restrict__ rows, int64_t nrows, int nq,
+                       unsigned long long *work, int32_t *sink) {
+    const int lane = threadIdx.x & 31;
+    uint32_t acc = 0;
+    for (;;) {
+        unsigned long long c = 0;
+        if (lane == 0) c = atomicAdd(work, (unsigned long long)kRowsInFlight);
+        const int64_t p0 = (int64_t)__shfl_sync(0xffffffffu, c, 0);
+        if (p0 >= nrows) break;
+        uint4 st[kRowsInFlight][2];
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            if (p0 + q < nrows) {
+                const uint4 *r = base + rows[p0 + q] * stride16;
+                if (lane < nq) st[q][0] = r[lane];
+                if (lane + 32 < nq) st[q][1] = r[lane + 32];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            if (p0 + q < nrows) {
+                if (lane < nq) acc ^= st[q][0].x ^ st[q][0].w;
+                if (lane + 32 < nq) acc ^= st[q][1].y;
+            }
+        }
+    }
+    if (acc == 0x9E3779B9u) atomicAdd(sink, 1);  // keeps the loads; practically never taken
+}
+
+ibp_status read_rows_probe(const void *base, int64_t stride_bytes, const int64_t *rows,
+                           int64_t nrows, int32_t read_bytes, void *ws, size_t ws_bytes,
+                           cudaStream_t st) {
+    if (!ws || ws_bytes < kStatusBytes) {
+        set_error("read_rows_probe: workspace of %zu bytes is below the required %zu", ws_bytes,
+                  kStatusBytes);
+        return IBP_ERR_WORKSPACE;
+    }
+    if (nrows <= 0) return IBP_OK;
+    int32_t *sink = reinterpret_cast<int32_t *>(ws);
+    auto *work = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(ws) + 64);
+    IBP_CUDA(cudaMemsetAsync(ws, 0, 128, st));
+    const int nq = (read_bytes + 15) / 16;
+    int per_sm = 0;
+    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, read_rows_probe_kernel,
+                                                           kFetchThreads, 0));
+    if (per_sm < 1) per_sm = 1;
+    if (per_sm > 2) per_sm = 2;  // the fetch kernel's residency
+    const int slot = profile_begin(st);
+    read_rows_probe_kernel<<<device_sm_count() * per_sm, kFetchThreads, 0, st>>>(
+        reinterpret_cast<const uint4 *>(base), stride_bytes / 16, rows, nrows, nq, work, sink);
+    IBP_LAUNCHED("read_rows_probe_kernel");
+    profile_end(slot, st);
     return IBP_OK;
 }
 

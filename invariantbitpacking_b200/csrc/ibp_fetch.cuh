@@ -349,39 +349,39 @@ __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables
         __syncwarp();
         if (qm) decode_rows_multi<U, NC>(slots, slot_words, qm, v, s.mw, lt, o);
         __syncwarp();
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int q = 0; q < kRowsInFlight; ++q) {
-        if (q < cnt) {
-            const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
-            U *o = reinterpret_cast<U *>(
-                __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
-            if (end[q] < 0) {
-                warp_copy<U>(o, s.comp + r * v, v);
-                continue;
-            }
-            if (end[q] >= v) {
-                // a bitmap claiming a stream as long as the raw row cannot come from this
-                // mask: report it and leave the output row alone
-                if (lane == 0) atomicOr(status, kStatusCorruptRow);
-                continue;
-            }
-            if (end[q] + 2 > slot_words) {
-                // longer than the slot (slots are sized for rows near the average length
-                // when rows are long): decode from the source row, whose words after the
-                // stream are its zero padding
-                decode_row<U, NC>(s.comp + r * v, v, s.mw, s.t, lt, o);
+        for (int q = 0; q < kRowsInFlight; ++q) {
+            if (q < cnt) {
+                const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
+                U *o = reinterpret_cast<U *>(
+                    __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
+                if (end[q] < 0) {
+                    warp_copy<U>(o, s.comp + r * v, v);
+                    continue;
+                }
+                if (end[q] >= v) {
+                    // a bitmap claiming a stream as long as the raw row cannot come from this
+                    // mask: report it and leave the output row alone
+                    if (lane == 0) atomicOr(status, kStatusCorruptRow);
+                    continue;
+                }
+                if (end[q] + 2 > slot_words) {
+                    // longer than the slot (slots are sized for rows near the average length
+                    // when rows are long): decode from the source row, whose words after the
+                    // stream are its zero padding
+                    decode_row<U, NC>(s.comp + r * v, v, s.mw, s.t, lt, o);
+                    __syncwarp();
+                    continue;
+                }
+                U *buf = slots + q * slot_words;
+                // words past the stream read as zero (get_bits looks one word ahead; the
+                // value there never reaches an output bit)
+                if (lane < 2) buf[end[q] + lane] = 0;
                 __syncwarp();
-                continue;
+                decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
+                __syncwarp();
             }
-            U *buf = slots + q * slot_words;
-            // words past the stream read as zero (get_bits looks one word ahead; the
-            // value there never reaches an output bit)
-            if (lane < 2) buf[end[q] + lane] = 0;
-            __syncwarp();
-            decode_row<U, NC>(buf, v, s.mw, s.t, lt, o);
-            __syncwarp();
         }
     }
 }
@@ -541,7 +541,6 @@ __device__ __forceinline__ void fetch_heads_exact(const RowSet<U> &s, const Lane
                                                   U *__restrict__ slots, int nslots,
                                                   int64_t slot_words, int64_t key, U *orow,
                                                   bool head, int32_t *status) {
-    constexpr int per16 = 16 / sizeof(U);
     const int lane = threadIdx.x & 31;
     const int64_t v = s.v;
     const int64_t raw_bytes = v * (int64_t)sizeof(U);

@@ -57,6 +57,10 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                            int nthreads, int impl, void *ws, size_t ws_bytes, cudaStream_t st,
                            const int64_t *offsets = nullptr, int64_t comp_bytes = 0);
 
+ibp_status read_rows_probe(const void *base, int64_t stride_bytes, const int64_t *rows,
+                           int64_t nrows, int32_t read_bytes, void *ws, size_t ws_bytes,
+                           cudaStream_t st);
+
 // ---- k-means (ibp_kmeans.cu)
 size_t kmeans_workspace(int64_t n, int64_t v, int wb, int c);
 template <typename U>

@@ -82,12 +82,14 @@ struct Server {
     std::vector<char *> tbl_host, tbl_dev;
     std::vector<bool> tbl_busy;
     std::vector<cudaEvent_t> tbl_event;  // completion event of the batch using each table
+    std::vector<cudaEvent_t> tbl_copied; // its index span and table are on the device
     void *ws = nullptr;
     size_t ws_bytes = 0;
     int64_t sort_cap = 0;  // rows a de-duplicating batch may hold (workspace size)
     int dedup = 0;         // 0: hashed batches, 1: sorted batches
     int64_t batch_rows = 0, batch_bytes = 0;  // admission limits of one batch
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;       // batch kernels, in launch order
+    cudaStream_t copy_stream = nullptr;  // index spans and tables, ahead of their kernels
     int device = 0;
 
     std::mutex mu;
@@ -95,6 +97,7 @@ struct Server {
     std::condition_variable done_cv;  // client waits
     std::condition_variable rec_cv;   // completion thread: a batch's event was recorded
     std::deque<int64_t> pending;
+    int64_t pending_bytes = 0;  // output bytes of the queued (not yet admitted) requests
     std::map<int64_t, SrvRequest> reqs;
     std::deque<Batch *> inflight;
     int64_t next_id = 1;
@@ -224,13 +227,18 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
     b->idx_end = s->idx_launched;
     std::vector<ibp_request> recs;
     int64_t rows = 0, out_bytes = 0;
+    // a backlog (requests arriving faster than the link drains them) is split over the
+    // launches that may be in flight, so batches grow with the queue: fewer, larger launches,
+    // and rows that several queued requests of one set share cross the bus once
+    const int64_t backlog_share = s->pending_bytes / std::max(1, s->max_inflight);
+    const int64_t byte_limit = std::max(s->batch_bytes, backlog_share);
     // admit in arrival order while the output fits (head-of-line: an oversized request
     // waits for memory, later ones wait behind it to keep arrival order) and the rows fit
     // one de-duplicating batch
     while (!s->pending.empty() && (int)recs.size() < s->max_batch) {
         SrvRequest &r = s->reqs[s->pending.front()];
         if (!recs.empty() &&
-            (rows + r.count > s->batch_rows || out_bytes + r.out_bytes > s->batch_bytes))
+            (rows + r.count > s->batch_rows || out_bytes + r.out_bytes > byte_limit))
             break;
         const int64_t off = arena_alloc(s, r.out_bytes);
         if (off < 0) break;
@@ -247,6 +255,7 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
         out_bytes += r.out_bytes;
         b->ids.push_back(r.id);
         b->idx_end = std::max(b->idx_end, r.ring_end);
+        s->pending_bytes -= r.out_bytes;
         s->pending.pop_front();
     }
     if (recs.empty()) {
@@ -263,21 +272,25 @@ static bool launch_batch_locked(Server *s, std::unique_lock<std::mutex> &lk) {
     // the GPU work needs no lock: the rings and tables it touches are reserved
     lk.unlock();
     cudaSetDevice(s->device);
-    // index span (one or two copies: the ring may have skipped to its start)
+    // index span (one or two copies: the ring may have skipped to its start) and the request
+    // table go on the copy stream, so they overlap the previous batch's kernel; the kernel
+    // waits for them.  Ring spans and tables of batches in flight never overlap.
     const int64_t lo = b->idx_begin % s->idx_cap, n = b->idx_end - b->idx_begin;
     if (n > 0) {
         if (lo + n <= s->idx_cap) {
             cudaMemcpyAsync(s->idx_dev + lo, s->idx_host + lo, sizeof(int64_t) * n,
-                            cudaMemcpyHostToDevice, s->stream);
+                            cudaMemcpyHostToDevice, s->copy_stream);
         } else {
             cudaMemcpyAsync(s->idx_dev + lo, s->idx_host + lo, sizeof(int64_t) * (s->idx_cap - lo),
-                            cudaMemcpyHostToDevice, s->stream);
+                            cudaMemcpyHostToDevice, s->copy_stream);
             cudaMemcpyAsync(s->idx_dev, s->idx_host, sizeof(int64_t) * (n - (s->idx_cap - lo)),
-                            cudaMemcpyHostToDevice, s->stream);
+                            cudaMemcpyHostToDevice, s->copy_stream);
         }
     }
     cudaMemcpyAsync(td, th, kTableHeader + sizeof(ibp_request) * recs.size(),
-                    cudaMemcpyHostToDevice, s->stream);
+                    cudaMemcpyHostToDevice, s->copy_stream);
+    cudaEventRecord(s->tbl_copied[table], s->copy_stream);
+    cudaStreamWaitEvent(s->stream, s->tbl_copied[table], 0);
     // a batch that fits the workspace is de-duplicated (hash claims inside the fetch, or a
     // radix sort); a single range request beyond it (distinct rows in order) goes as listed
     const ibp_request *dreq = reinterpret_cast<const ibp_request *>(td + kTableHeader);
@@ -317,11 +330,14 @@ static void release_server(Server *s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (char *h : s->tbl_host) cudaFreeHost(h);
     for (char *d : s->tbl_dev) cudaFree(d);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (cudaEvent_t ev : s->tbl_event) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : s->tbl_copied) cudaEventDestroy(ev);
     if (s->idx_host) cudaFreeHost(s->idx_host);
     if (s->idx_dev) cudaFree(s->idx_dev);
     if (s->ws) cudaFree(s->ws);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     for (Batch *b : s->inflight) delete b;
     delete s;
 }
@@ -363,6 +379,7 @@ ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int
     };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "copy stream");
     if ((e = cudaHostAlloc(&s->idx_host, sizeof(int64_t) * index_capacity, cudaHostAllocDefault)) != cudaSuccess) return fail(e, "index staging");
     if ((e = cudaMalloc(&s->idx_dev, sizeof(int64_t) * index_capacity)) != cudaSuccess) return fail(e, "device index ring");
     const size_t tbytes = kTableHeader + sizeof(ibp_request) * max_batch;
@@ -376,6 +393,9 @@ ibp_status ibp_server_create(const void *registry, const ibp_set_desc *sets, int
         cudaEvent_t ev = nullptr;
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
         s->tbl_event.push_back(ev);
+        cudaEvent_t cev = nullptr;
+        if ((e = cudaEventCreateWithFlags(&cev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+        s->tbl_copied.push_back(cev);
     }
     s->sort_cap = std::min<int64_t>(std::max<int64_t>(index_capacity, 1 << 20), INT32_MAX);
     s->batch_rows = s->sort_cap;
@@ -432,6 +452,7 @@ ibp_status ibp_server_submit(ibp_server *srv, int32_t set, const int64_t *rows, 
     r.ring_end = s->idx_head;
     s->reqs[r.id] = r;
     s->pending.push_back(r.id);
+    s->pending_bytes += r.out_bytes;
     *id = r.id;
     lk.unlock();
     s->cv.notify_all();
@@ -488,7 +509,10 @@ ibp_status ibp_server_cancel(ibp_server *srv, int64_t id) {
             return IBP_ERR_UNSUPPORTED;
         }
         auto p = std::find(s->pending.begin(), s->pending.end(), id);
-        if (p != s->pending.end()) s->pending.erase(p);
+        if (p != s->pending.end()) {
+            s->pending.erase(p);
+            s->pending_bytes -= it->second.out_bytes;
+        }
         s->reqs.erase(it);
     }
     s->cv.notify_all();
