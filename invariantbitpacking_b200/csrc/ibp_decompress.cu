@@ -175,10 +175,12 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
     int64_t seen = 0;  // positions handed out when this warp last took a chunk
     for (;;) {
         // guided self-scheduling: 32-position chunks while much work remains, shrinking to
-        // 4 towards the end, so that the grid's last chunks (each a chain of dependent
-        // reads) finish close together
+        // 4 towards the end (fewer when the fetch is small enough to give every warp less),
+        // so that the grid's last chunks (each a chain of dependent reads) finish close
+        // together
         const int g = (int)min((int64_t)a.gmax,
-                               max((int64_t)min(4, a.gmax), (nrows - seen) / (2 * nwarps)));
+                               max((int64_t)min(min(4, a.gmax), a.upos),
+                                   (nrows - seen) / (2 * nwarps)));
         unsigned long long c = 0;
         if (lane == 0) c = atomicAdd(a.work, (unsigned long long)g);
         const int64_t p0 = (int64_t)__shfl_sync(0xffffffffu, c, 0);

@@ -13,11 +13,12 @@ constexpr int kRowsInFlight = 4;  // first reads a warp keeps outstanding
 
 // Positions a warp takes per unit of work: 32 (lane-parallel metadata over the full warp)
 // unless the fetch has too few rows to give every warp of the grid a unit; then fewer, down
-// to 4, so a small fetch spreads over more warps (each warp's rows form a chain of dependent
-// reads, a few microseconds each over PCIe).
+// to 1, so a small fetch spreads over more warps and SMs (each warp's rows form a chain of
+// dependent reads, a few microseconds each over PCIe, and an SM keeps a limited number of
+// host reads in flight).
 __host__ __device__ __forceinline__ int unit_positions(int64_t rows, int64_t warps) {
     int u = 32;
-    while (u > 4 && (int64_t)(u / 2) * warps >= rows) u >>= 1;
+    while (u > 1 && (int64_t)(u / 2) * warps >= rows) u >>= 1;
     return u;
 }
 
@@ -279,11 +280,31 @@ __device__ __forceinline__ int64_t row_words(const U *__restrict__ buf, int64_t 
 // bitmaps, the rest of every row that needs more than its first read (all issued before any
 // is waited for: 16-byte blocks in registers, at most 32 per row; longer tails and
 // unaligned rows take the plain loop), then the decode (or copy, for rows stored raw).
+// A row stored raw (not packed) is copied to its output from its slot when the caller staged
+// it there whole (raw_staged), else straight from its source.
+template <typename U>
+__device__ __forceinline__ void copy_raw_row(U *o, const U *slot, const U *src, int64_t v,
+                                             bool raw_staged) {
+    if (raw_staged) {
+        const int lane = threadIdx.x & 31;
+        if ((((uintptr_t)o) & 15) == 0) {
+            const int64_t n16 = v * (int64_t)sizeof(U) / 16;
+            for (int64_t k = lane; k < n16; k += 32)
+                reinterpret_cast<uint4 *>(o)[k] = reinterpret_cast<const uint4 *>(slot)[k];
+        } else {
+            for (int64_t k = lane; k < v; k += 32) o[k] = slot[k];
+        }
+    } else {
+        warp_copy<U>(o, src, v);
+    }
+}
+
 template <typename U, int NC, bool MULTI = false>
 __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables<U, NC> &lt,
                                             U *__restrict__ slots, int64_t slot_words,
                                             const int *lid, int cnt, int64_t key, U *orow,
-                                            bool packed, int32_t *status) {
+                                            bool packed, int32_t *status,
+                                            bool raw_staged = false) {
     const int lane = threadIdx.x & 31;
     const int64_t v = s.v;
     int64_t end[kRowsInFlight];
@@ -334,7 +355,7 @@ __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables
                 o[q] = reinterpret_cast<U *>(
                     __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
                 if (end[q] < 0) {
-                    warp_copy<U>(o[q], s.comp + r * v, v);
+                    copy_raw_row<U>(o[q], slots + q * slot_words, s.comp + r * v, v, raw_staged);
                 } else if (end[q] >= v) {
                     if (lane == 0) atomicOr(status, kStatusCorruptRow);
                 } else if (end[q] + 2 > slot_words) {  // not with slots of v + 2 words
@@ -357,7 +378,7 @@ __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables
                 U *o = reinterpret_cast<U *>(
                     __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(orow), lid[q]));
                 if (end[q] < 0) {
-                    warp_copy<U>(o, s.comp + r * v, v);
+                    copy_raw_row<U>(o, slots + q * slot_words, s.comp + r * v, v, raw_staged);
                     continue;
                 }
                 if (end[q] >= v) {
@@ -397,8 +418,15 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
                                             U *__restrict__ slots, int nslots,
                                             int64_t slot_words, int64_t key, U *orow,
                                             bool head, bool packed, int32_t *status) {
+    constexpr int per16 = 16 / sizeof(U);
     const int lane = threadIdx.x & 31;
     const int64_t v = s.v;
+    // rows stored raw are read whole into their slot together with the other rows' first
+    // reads when they fit it and the register staging, so copying them out costs no round
+    // trip of its own
+    const int64_t nq_raw = v / per16;
+    const bool raw_staged = (v % per16) == 0 && v + 2 <= slot_words && nq_raw <= 64 &&
+                            (((uintptr_t)s.comp) & 15) == 0;
     unsigned hm = __ballot_sync(0xffffffffu, head);
     while (hm) {
         int lid[kRowsInFlight];
@@ -413,22 +441,24 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
             }
         }
         {
-            constexpr int per16 = 16 / sizeof(U);
             const int64_t nq = (s.first_words + per16 - 1) / per16;
             uint4 stage[kRowsInFlight][2];
-            bool fast[kRowsInFlight];
+            unsigned fastm = 0, rawm = 0;  // bit q: staged in registers; row q stored raw
 #pragma unroll
             for (int q = 0; q < kRowsInFlight; ++q) {
-                fast[q] = false;
                 if (q < cnt) {
                     const int64_t r = __shfl_sync(0xffffffffu, key, lid[q]);
                     const bool pk = __shfl_sync(0xffffffffu, (int)packed, lid[q]);
                     const U *row = s.comp + r * v;
-                    fast[q] = pk && ((((uintptr_t)row) & 15) == 0) && nq <= 64;
-                    if (fast[q]) {
+                    const int64_t n = pk ? nq : nq_raw;
+                    const bool fast = (pk || raw_staged) && ((((uintptr_t)row) & 15) == 0) &&
+                                      n <= 64;
+                    fastm |= (unsigned)fast << q;
+                    rawm |= (unsigned)!pk << q;
+                    if (fast) {
                         const uint4 *r4 = reinterpret_cast<const uint4 *>(row);
-                        if (lane < nq) stage[q][0] = r4[lane];
-                        if (lane + 32 < nq) stage[q][1] = r4[lane + 32];
+                        if (lane < n) stage[q][0] = r4[lane];
+                        if (lane + 32 < n) stage[q][1] = r4[lane + 32];
                     } else if (pk) {
                         issue_words<U>(slots + q * slot_words, row, 0, s.first_words);
                     }
@@ -436,15 +466,17 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
             }
 #pragma unroll
             for (int q = 0; q < kRowsInFlight; ++q) {
-                if (fast[q]) {
+                if ((fastm >> q) & 1) {
+                    const int64_t n = ((rawm >> q) & 1) ? nq_raw : nq;
                     uint4 *b4 = reinterpret_cast<uint4 *>(slots + q * slot_words);
-                    if (lane < nq) b4[lane] = stage[q][0];
-                    if (lane + 32 < nq) b4[lane + 32] = stage[q][1];
+                    if (lane < n) b4[lane] = stage[q][0];
+                    if (lane + 32 < n) b4[lane + 32] = stage[q][1];
                 }
             }
         }
         __syncwarp();
-        finish_rows<U, NC>(s, lt, slots, slot_words, lid, cnt, key, orow, packed, status);
+        finish_rows<U, NC>(s, lt, slots, slot_words, lid, cnt, key, orow, packed, status,
+                           raw_staged);
     }
 }
 
