@@ -528,6 +528,12 @@ def served_summary(line):
     for e in line["rates"]:
         srv, own = e["served"], e["per_request"]
         ref = e.get("per_request_reference")
+        # requests per second each arm completes without a growing queue: its delivered
+        # bytes per second over the mean request's output
+        mean_req = e["output_GB"] * 1e9 / e["requests"]
+        for arm in (srv, own, ref):
+            if arm is not None:
+                arm["sustainable_rate_per_s"] = round(arm["GBps"] * 1e9 / mean_req, 1)
         row = {"rate_per_s": e["rate_per_s"], "requests": e["requests"],
                "served": srv, "per_request": own,
                "served_beats_per_request": bool(srv["GBps"] >= own["GBps"]
@@ -1820,7 +1826,7 @@ def main():
             except Exception as exc:  # reported, not fatal
                 line["plain_small"] = {"error": repr(exc)[:300]}
             line["served_mix"] = served_summary(subconfig_line(
-                "served_mix", ["--rates", "2000,20000", "--requests", "150"], 900))
+                "served_mix", ["--rates", "1000,2000,20000", "--requests", "150"], 900))
             line["embedding_tables"] = batched_summary(subconfig_line(
                 "embedding_tables", ["--steps", "20", "--warmup", "3"], 900))
             line["decoder_layer"] = batched_summary(subconfig_line(

@@ -94,10 +94,12 @@ __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
 // appended to `heads` (one atomic per block and pass, so the list's counter is not a hot
 // spot), and the fetch kernel then walks distinct rows only, 32 to a chunk.  Out-of-range
 // rows are flagged here and never claimed.  256 threads per block, one position each.
+// records: each listed head is two words, its position and its row, so that a fetch reads
+// one 16-byte record per row instead of a position and then the index entry it points to.
 __global__ void __launch_bounds__(256)
 claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int64_t *hkeys,
                    int64_t *hpos, int64_t hslots, int64_t *__restrict__ heads,
-                   unsigned long long *nheads, int32_t *status) {
+                   unsigned long long *nheads, int32_t *status, bool records) {
     __shared__ unsigned counts[8];
     __shared__ unsigned long long block_base;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -124,7 +126,9 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
             block_base = run ? atomicAdd(nheads, (unsigned long long)run) : 0ull;
         }
         __syncthreads();
-        if (head) heads[block_base + counts[wid] + __popc(hm & ((1u << lane) - 1u))] = k;
+        const unsigned long long at = block_base + counts[wid] + __popc(hm & ((1u << lane) - 1u));
+        if (head && !records) heads[at] = k;
+        if (head && records) reinterpret_cast<longlong2 *>(heads)[at] = make_longlong2(k, key);
         __syncthreads();  // counts and block_base are rewritten by the next pass
     }
 }
@@ -371,8 +375,12 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
         if (p0 >= nrows) break;
         const int avail = (int)min((int64_t)chunk, nrows - p0);
         const bool valid = lane < avail;
-        const int64_t k = valid ? (a.list ? a.list[p0 + lane] : p0 + lane) : 0;
-        const int64_t key = valid ? (a.keys ? a.keys[k] : k) : 0;
+        int64_t k = p0 + lane, key = k;
+        if (valid && a.list) {  // a head record of the claim pass: position and row
+            const longlong2 r = reinterpret_cast<const longlong2 *>(a.list)[p0 + lane];
+            k = r.x;
+            key = r.y;
+        }
         const bool bad = valid && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         const bool ok = valid && !bad;
@@ -422,7 +430,7 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
 template <typename U>
 static bool hbm_rows_fit(const FetchArgs<U> &a) {
     return a.device_rows && !a.raw_only && !a.dedup && !a.pos && !a.s.offsets &&
-           !a.claims.keys && a.s.v <= 64 &&
+           !a.claims.keys && (!a.keys || a.list) && a.s.v <= 64 &&
            (a.s.v * (int64_t)sizeof(U)) % 16 == 0 && (((uintptr_t)a.s.comp) & 15) == 0;
 }
 
@@ -509,7 +517,7 @@ size_t decompress_workspace(int64_t nidx, int64_t v, int wb, bool has_index) {
         Sizer hsh;
         hsh.take<int64_t>(hash_slots(nidx));
         hsh.take<int64_t>(hash_slots(nidx));
-        hsh.take<int64_t>(nidx);  // claimed heads
+        hsh.take<int64_t>(2 * nidx);  // claimed heads (records of two words)
         s.take<char>(std::max(srt.total(), hsh.total()));
     }
     return s.total();
@@ -663,7 +671,7 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         const int64_t slots = hash_slots(nidx);
         int64_t *hkeys = c.take<int64_t>(slots);
         int64_t *hpos = c.take<int64_t>(slots);
-        int64_t *heads = c.take<int64_t>(nidx);
+        int64_t *heads = c.take<int64_t>(2 * nidx);
         // keys -1 (empty); positions -1 (unpublished) for the in-fetch claims
         IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, (char *)(hpos + slots) - (char *)hkeys, st));
         a.keys = idx;
@@ -674,11 +682,13 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                 reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 128);
             const int64_t cb =
                 std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
-            claim_heads_kernel<<<(unsigned)cb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
-                                                             heads, nheads, status);
-            IBP_LAUNCHED("claim_heads_kernel");
             a.list = heads;
             a.list_len = nheads;
+            // the HBM-row kernel reads head records (position, row)
+            const bool records = hbm_rows_fit(a);
+            claim_heads_kernel<<<(unsigned)cb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
+                                                             heads, nheads, status, records);
+            IBP_LAUNCHED("claim_heads_kernel");
         } else {
             // host rows: claims and repeat copies happen inside the fetch, hidden behind its
             // PCIe reads
