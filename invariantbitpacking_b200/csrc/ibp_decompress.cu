@@ -238,13 +238,14 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
 
 // ------------------------------------------------------------------ HBM rows of <= 64 words
 // Rows in device memory are not bound by a link but by the instructions around the decode,
-// so this kernel keeps per-row bookkeeping to a minimum: a warp takes 32 listed rows (the
-// claim pass's distinct rows, or rows p .. p+31 of an unindexed fetch), parks their keys and
-// output rows in shared memory, and copies groups of G whole rows (one 16-byte cp.async per
-// lane and row; rows must be 16-byte aligned) into one of two shared buffers while it
-// decodes the previous group from the other.  A group's prefix sums are issued together;
-// the row's stream length falls out of them (no separate length pass, no tail reads), and
-// stream offsets are 32-bit.
+// so this kernel keeps per-row bookkeeping to a minimum: a warp takes a chunk of listed rows
+// from a work counter (the claim pass's head records -- position and row -- or rows p, p+1,
+// ... of an unindexed fetch; 4 rows at a time unless every warp gets several chunks of 32),
+// parks their keys and output rows in shared memory, and copies groups of G whole rows (one
+// 16-byte cp.async per lane and row; rows must be 16-byte aligned) into one of two shared
+// buffers while it decodes the previous group from the other.  A group's prefix sums are
+// issued together; the row's stream length falls out of them (no separate length pass, no
+// tail reads), and stream offsets are 32-bit.
 template <typename U>
 __device__ __forceinline__ U stream_bits(const U *words, uint32_t s, int L) {
     constexpr int W = 8 * sizeof(U);

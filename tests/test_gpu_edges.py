@@ -357,3 +357,26 @@ def test_corrupt_rows_are_flagged_and_skipped(ibp, oracle, where, wb, v):
         keep = ~skip
         want = oracle.decompress(comp, m, b, bad_bits.view(np.int32), rows[keep])
         assert same(got[keep], want.view(d.dtype))
+
+
+def test_read_rows_probe_reads_the_listed_rows(ibp):
+    """The access-pattern probe (a measurement aid) runs over host and device rows, takes
+    every listed row (its work counter ends at or past the list), and refuses reads that would
+    leave a row's stride."""
+    from invariantbitpacking_b200 import _capi
+    lib = _capi.lib
+    n, v = 5000, 64
+    x = torch.zeros((n, v), dtype=torch.int64).pin_memory()
+    rows = torch.randint(0, n, (3000,), device="cuda")
+    ws = torch.zeros(256, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for base in (x, x.cuda()):
+        for nbytes in (16, 288, 512):
+            _capi.check(lib.ibp_read_rows_probe(base.data_ptr(), v * 8, rows.data_ptr(), 3000,
+                                                nbytes, ws.data_ptr(), 256, st))
+            torch.cuda.synchronize()
+            assert int(ws[64:72].view(torch.int64).item()) >= 3000
+    assert lib.ibp_read_rows_probe(x.data_ptr(), v * 8, rows.data_ptr(), 3000, 600, ws.data_ptr(),
+                                   256, st) == _capi.IBP_ERR_ARGUMENT
+    assert lib.ibp_read_rows_probe(x.data_ptr(), v * 8, rows.data_ptr(), 3000, 288, ws.data_ptr(),
+                                   16, st) == _capi.IBP_ERR_WORKSPACE
