@@ -286,10 +286,8 @@ static ibp_status launch_batch_nc(BatchArgs<U> a, int64_t max_v, Shape sh, cudaS
     }
     a.slots = slots;
     auto kern = batch_fetch_kernel<U, NC>;
-    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-    if (per_sm < 1) per_sm = 1;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, threads, smem, &per_sm));
     if (sh.occupancy > 0 && sh.occupancy < per_sm) per_sm = sh.occupancy;
     const int blocks = device_sm_count() * per_sm;
     const int slot = profile_begin(st);
@@ -534,10 +532,8 @@ static ibp_status launch_sorted_nc(SortedArgs<U> a, int64_t max_v, Shape sh, cud
     }
     a.slots = slots;
     auto kern = batch_fetch_sorted_kernel<U, NC>;
-    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-    if (per_sm < 1) per_sm = 1;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, threads, smem, &per_sm));
     if (sh.occupancy > 0 && sh.occupancy < per_sm) per_sm = sh.occupancy;
     const int pslot = profile_begin(st);
     kern<<<device_sm_count() * per_sm, threads, smem, st>>>(a);
@@ -776,10 +772,8 @@ static ibp_status launch_hashed(const void *reg, const RegistryHeader &h, const 
     }
     a.warp_words = warp_words;
     auto kern = batch_fetch_hashed_kernel<U>;
-    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-    if (per_sm < 1) per_sm = 1;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, threads, smem, &per_sm));
     if (sh.occupancy > 0 && sh.occupancy < per_sm) per_sm = sh.occupancy;
     const int pslot = profile_begin(st);
     kern<<<device_sm_count() * per_sm, threads, smem, st>>>(a);

@@ -89,6 +89,53 @@ static DevInfo &dev_info() {
 int device_sm_count() { return dev_info().sms; }
 int device_max_smem_optin() { return dev_info().smem_optin; }
 
+// Per device and kernel: the dynamic shared-memory limit set so far, and the resident blocks
+// per SM of each launch shape asked for (a per-call fetch of a few thousand rows spends
+// microseconds of host time on these queries otherwise).
+ibp_status kernel_blocks_per_sm(const void *kern, int threads, size_t smem, int *per_sm) {
+    struct Shape {
+        int dev;
+        const void *kern;
+        int threads;
+        size_t smem;
+        int per_sm;
+    };
+    struct Limit {
+        int dev;
+        const void *kern;
+        size_t smem;
+    };
+    static std::mutex mu;
+    static std::vector<Shape> shapes;
+    static std::vector<Limit> limits;
+    int dev = 0;
+    IBP_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    for (const Shape &s : shapes)
+        if (s.dev == dev && s.kern == kern && s.threads == threads && s.smem == smem) {
+            *per_sm = s.per_sm;
+            return IBP_OK;
+        }
+    Limit *lim = nullptr;
+    for (Limit &l : limits)
+        if (l.dev == dev && l.kern == kern) lim = &l;
+    if (!lim) {
+        limits.push_back({dev, kern, 48 * 1024});
+        lim = &limits.back();
+    }
+    if (smem > lim->smem) {
+        IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        lim->smem = smem;
+    }
+    int n = 0;
+    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem));
+    if (n < 1) n = 1;
+    shapes.push_back({dev, kern, threads, smem, n});
+    *per_sm = n;
+    return IBP_OK;
+}
+
 static bool on_host(const void *p) {
     cudaPointerAttributes pa{};
     if (cudaPointerGetAttributes(&pa, p) != cudaSuccess) {

@@ -103,17 +103,24 @@ __device__ __forceinline__ U scatter_bits(U y, U sel, const U *mv, int stride) {
     return (U)(y & sel);
 }
 
+// Column j of the tables.
+template <typename U>
+__device__ __forceinline__ void build_table_column(const U *__restrict__ mask,
+                                                   const U *__restrict__ bitval, int64_t v,
+                                                   const ColTables<U> &t, int64_t j) {
+    const U m = mask[j];
+    t.mask[j] = m;
+    t.bitval[j] = bitval[j];
+    t.nb[j] = (uint8_t)(8 * sizeof(U) - popc_w(m));
+    move_masks<U>((U)~m, t.mv + j, (int)v);
+}
+
 template <typename U>
 __global__ void build_tables_kernel(const U *__restrict__ mask, const U *__restrict__ bitval,
                                     int64_t v, ColTables<U> t) {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < v;
-         j += (int64_t)gridDim.x * blockDim.x) {
-        const U m = mask[j];
-        t.mask[j] = m;
-        t.bitval[j] = bitval[j];
-        t.nb[j] = (uint8_t)(8 * sizeof(U) - popc_w(m));
-        move_masks<U>((U)~m, t.mv + j, (int)v);
-    }
+         j += (int64_t)gridDim.x * blockDim.x)
+        build_table_column<U>(mask, bitval, v, t, j);
 }
 
 template <typename U>

@@ -108,6 +108,10 @@ struct Sizer {
 
 int device_sm_count();        // SMs of the current device (cached per device)
 int device_max_smem_optin();  // opt-in shared memory per block (cached per device)
+// Resident blocks per SM (at least 1) of a kernel launched with `threads` and `smem` bytes of
+// dynamic shared memory on the current device, after raising the kernel's dynamic
+// shared-memory limit to `smem` when needed; cached per device, kernel and shape.
+ibp_status kernel_blocks_per_sm(const void *kern, int threads, size_t smem, int *per_sm);
 
 // ------------------------------------------------------------------ word helpers
 template <typename U>

@@ -231,10 +231,8 @@ static ibp_status launch_pack(PackArgs<U> a, cudaStream_t st) {
         return IBP_ERR_UNSUPPORTED;
     }
     auto kern = pack_rows_kernel<U>;
-    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, smem));
-    if (per_sm < 1) per_sm = 1;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, wpb * 32, smem, &per_sm));
     int64_t blocks = (a.nrows + wpb - 1) / wpb;
     const int64_t cap = (int64_t)device_sm_count() * per_sm;
     if (blocks > cap) blocks = cap;

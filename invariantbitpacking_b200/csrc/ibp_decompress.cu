@@ -69,39 +69,30 @@ struct FetchArgs {
 
 // ------------------------------------------------------------------ hashed dedup
 // (row_hash, hash_claim_slot and the in-fetch claim helpers are in ibp_fetch.cuh)
-__device__ __forceinline__ bool hash_claim(int64_t *keys, int64_t *pos, int64_t slots,
-                                           int64_t key, int64_t k) {
-    bool won;
-    const int64_t h = hash_claim_slot(keys, slots, key, won);
-    if (won) pos[h] = k;
-    return won;
-}
-
-__device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
-                                             const int64_t *__restrict__ pos, int64_t slots,
-                                             int64_t key) {
-    uint64_t h = row_hash(key, slots);
-    for (int64_t probe = 0; probe < slots; ++probe) {
-        const int64_t kk = keys[h];
-        if (kk == key) return pos[h];
-        if (kk == -1) return -1;
-        h = h + 1 == (uint64_t)slots ? 0 : h + 1;
-    }
-    return -1;
-}
+constexpr uint64_t kRecordPacked = 1ull << 63;  // head record: the row is stored compressed
 
 // Claim pass of a hashed fetch: every position claims its row; the positions that win are
 // appended to `heads` (one atomic per block and pass, so the list's counter is not a hot
 // spot), and the fetch kernel then walks distinct rows only, 32 to a chunk.  Out-of-range
 // rows are flagged here and never claimed.  256 threads per block, one position each.
-// records: each listed head is two words, its position and its row, so that a fetch reads
-// one 16-byte record per row instead of a position and then the index entry it points to.
+// bitmask != nullptr: each listed head is a record of two words, its position (bit 63 set
+// when the row is stored compressed) and its row, so that a fetch reads one 16-byte record
+// per row instead of a position, then the index entry it points to, then the bitmask word.
 __global__ void __launch_bounds__(256)
 claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int64_t *hkeys,
                    int64_t *hpos, int64_t hslots, int64_t *__restrict__ heads,
-                   unsigned long long *nheads, int32_t *status, bool records) {
+                   unsigned long long *nheads, int32_t *status,
+                   const int32_t *__restrict__ bitmask) {
+    const bool records = bitmask != nullptr;
     __shared__ unsigned counts[8];
     __shared__ unsigned long long block_base;
+    // the block's own table of the rows its 256 positions hold (empty: ~0), so that a hot row
+    // of a skewed batch is claimed once per block: every claim of one row reads the same
+    // global slot, which one L2 slice serves
+    constexpr int kBlockSlots = 512;
+    __shared__ unsigned long long btab[kBlockSlots];
+    for (int i = threadIdx.x; i < kBlockSlots; i += 256) btab[i] = ~0ull;
+    __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int64_t b0 = (int64_t)blockIdx.x * 256; b0 < nidx; b0 += (int64_t)gridDim.x * 256) {
         const int64_t k = b0 + threadIdx.x;
@@ -109,10 +100,28 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
         const bool bad = k < nidx && (key < 0 || key >= n);
         if (bad) atomicOr(status, kStatusBadIndex);
         const bool ok = k < nidx && !bad;
+        // the row's bitmask word, loaded before the claim so that the two latencies overlap
+        const int32_t bmw = records && ok ? __ldg(&bitmask[key >> 5]) : 0;
         // one claim per distinct row of the warp (the lowest lane holding it)
         const unsigned same = __match_any_sync(0xffffffffu, ok ? key : (int64_t)-1);
-        const bool first = ok && (__ffs(same) - 1) == lane;
-        const bool head = first && hash_claim(hkeys, hpos, hslots, key, k);
+        bool lead = ok && (__ffs(same) - 1) == lane;
+        if (lead) {
+            uint32_t h = (uint32_t)row_hash(key, kBlockSlots);
+            for (int probe = 0; probe < kBlockSlots; ++probe) {
+                const unsigned long long old = atomicCAS(&btab[h], ~0ull, (unsigned long long)key);
+                if (old == ~0ull) break;  // the block's first position of this row
+                if (old == (unsigned long long)key) {
+                    lead = false;
+                    break;
+                }
+                h = (h + 1) & (kBlockSlots - 1);
+            }
+        }
+        bool head = false;
+        if (lead) {
+            const int64_t slot = hash_claim_slot(hkeys, hslots, key, head);
+            if (head) hpos[slot] = k;
+        }
         const unsigned hm = __ballot_sync(0xffffffffu, head);
         if (lane == 0) counts[wid] = __popc(hm);
         __syncthreads();
@@ -128,16 +137,40 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
         __syncthreads();
         const unsigned long long at = block_base + counts[wid] + __popc(hm & ((1u << lane) - 1u));
         if (head && !records) heads[at] = k;
-        if (head && records) reinterpret_cast<longlong2 *>(heads)[at] = make_longlong2(k, key);
-        __syncthreads();  // counts and block_base are rewritten by the next pass
+        if (head && records) {
+            const bool packed = (bmw >> (key & 31)) & 1;
+            reinterpret_cast<longlong2 *>(heads)[at] =
+                make_longlong2(packed ? (int64_t)((uint64_t)k | kRecordPacked) : k, key);
+        }
+        for (int i = threadIdx.x; i < kBlockSlots; i += 256) btab[i] = ~0ull;
+        __syncthreads();  // counts, block_base and btab are rewritten by the next pass
     }
 }
 
 // Repeats of a hashed fetch whose claims came from claim_heads_kernel: each position whose
 // row another position claimed copies that position's output row (copy_rows, four rows at
-// a time per warp).
+// a time per warp).  The rows it copies were written by the fetch kernel before it, so they
+// are read through L1: the hot rows of a skewed batch then leave L2 once per SM rather than
+// once per copy (one L2 slice holds each 128-byte line of a row, and a Zipf(1.1) batch of
+// 400k positions copies its hottest row ~40k times); the claim table, written by the claim
+// pass, is read the same way.
+constexpr int kFillThreads = 256;
+
+__device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
+                                             const int64_t *__restrict__ pos, int64_t slots,
+                                             int64_t key) {
+    uint64_t h = row_hash(key, slots);
+    for (int64_t probe = 0; probe < slots; ++probe) {
+        const int64_t kk = __ldg(&keys[h]);
+        if (kk == key) return __ldg(&pos[h]);
+        if (kk == -1) return -1;
+        h = h + 1 == (uint64_t)slots ? 0 : h + 1;
+    }
+    return -1;
+}
+
 template <typename U>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kFillThreads)
 fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
                    const int64_t *__restrict__ hkeys, const int64_t *__restrict__ hpos,
                    int64_t hslots, U *__restrict__ out, int64_t v) {
@@ -151,9 +184,24 @@ fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
         int64_t hp = -1;
         if (key >= 0 && key < n) hp = hash_find(hkeys, hpos, hslots, key);
         const bool rep = hp >= 0 && hp != k;
-        copy_rows<U>(__ballot_sync(0xffffffffu, rep), out + (rep ? hp : 0) * v,
-                     out + (rep ? k : 0) * v, v, vec_rows);
+        copy_rows<U, true>(__ballot_sync(0xffffffffu, rep), out + (rep ? hp : 0) * v,
+                           out + (rep ? k : 0) * v, v, vec_rows);
     }
+}
+
+// One wave of resident blocks, each warp striding over chunks of 32 positions.
+template <typename U>
+static ibp_status launch_fill_hashed(const int64_t *idx, int64_t nidx, int64_t n,
+                                     const int64_t *hkeys, const int64_t *hpos, int64_t slots,
+                                     U *out, int64_t v, cudaStream_t st) {
+    auto kern = fill_hashed_kernel<U>;
+    int per_sm = 0;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, kFillThreads, 0, &per_sm));
+    const int64_t fb = std::min<int64_t>((nidx + kFillThreads - 1) / kFillThreads,
+                                         (int64_t)device_sm_count() * per_sm);
+    kern<<<(unsigned)fb, kFillThreads, 0, st>>>(idx, nidx, n, hkeys, hpos, slots, out, v);
+    IBP_LAUNCHED("fill_hashed_kernel");
+    return IBP_OK;
 }
 
 // ------------------------------------------------------------------ fetch kernel
@@ -239,13 +287,15 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
 // ------------------------------------------------------------------ HBM rows of <= 64 words
 // Rows in device memory are not bound by a link but by the instructions around the decode,
 // so this kernel keeps per-row bookkeeping to a minimum: a warp takes a chunk of listed rows
-// from a work counter (the claim pass's head records -- position and row -- or rows p, p+1,
-// ... of an unindexed fetch; 4 rows at a time unless every warp gets several chunks of 32),
-// parks their keys and output rows in shared memory, and copies groups of G whole rows (one
-// 16-byte cp.async per lane and row; rows must be 16-byte aligned) into one of two shared
-// buffers while it decodes the previous group from the other.  A group's prefix sums are
-// issued together; the row's stream length falls out of them (no separate length pass, no
-// tail reads), and stream offsets are 32-bit.
+// from a work counter (the claim pass's head records -- position with the row's
+// stored-compressed flag, and row -- or rows p, p+1, ... of an unindexed fetch; 4 to 32 rows
+// at a time by the batch's size), parks their keys and output rows in shared memory, and
+// copies groups of G whole rows (one 16-byte cp.async per lane and row; rows must be 16-byte
+// aligned) into one of two shared buffers while it decodes the previous group from the
+// other.  A group whose words are all compressible (the usual case: a good mask leaves few
+// words whole) takes its stream offsets from a table made once per warp; otherwise its prefix
+// sums are issued together.  The row's stream length falls out of the offsets (no separate
+// length pass, no tail reads), and stream offsets are 32-bit.
 template <typename U>
 __device__ __forceinline__ U stream_bits(const U *words, uint32_t s, int L) {
     constexpr int W = 8 * sizeof(U);
@@ -274,15 +324,19 @@ __device__ __forceinline__ U stream_bits_funnel(const U *words, uint32_t s, int 
     }
 }
 
+// `full[32 * c + lane]`: the inclusive prefix over the lanes of chunk c of the kept bits of
+// every column (the stream offsets of a row whose words are all compressible).
 template <typename U, int NC, int G>
 __device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int sw, int r0,
                                                  int rows, unsigned okm, unsigned pm, int v,
                                                  int mw, const LaneTables<U, NC> &lt,
-                                                 U *const *mout, int32_t *status) {
+                                                 const uint32_t *full, U *const *mout,
+                                                 int32_t *status) {
     constexpr int W = 8 * sizeof(U);
     const int lane = threadIdx.x & 31;
     uint32_t incl[G][NC];
     unsigned cjm = 0;  // bit q * NC + c: this lane's column of chunk c in row q is compressible
+    bool mixed = false;  // a packed row of the group has a word stored whole
 #pragma unroll
     for (int q = 0; q < G; ++q) {
         const int r = r0 + q;
@@ -293,17 +347,31 @@ __device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int 
             const bool in = 32 * c + lane < v;
             const bool cj = pk && in && ((units[c] >> lane) & 1u);
             cjm |= (unsigned)cj << (q * NC + c);
-            incl[q][c] = (pk && in) ? (cj ? (uint32_t)lt.nb[c] : (uint32_t)W) : 0u;
+            mixed |= pk && in && !cj;
+            incl[q][c] = pk ? full[c * 32 + lane] : 0u;
         }
     }
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
+    if (__any_sync(0xffffffffu, mixed)) {
+        // some word of the group is stored whole: offsets from a prefix sum per row and chunk
 #pragma unroll
         for (int q = 0; q < G; ++q) {
+            const bool pk = r0 + q < rows && ((pm >> (r0 + q)) & 1);
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl[q][c], off);
-                if (lane >= off) incl[q][c] += y;
+                const bool in = 32 * c + lane < v;
+                const bool cj = (cjm >> (q * NC + c)) & 1u;
+                incl[q][c] = (pk && in) ? (cj ? (uint32_t)lt.nb[c] : (uint32_t)W) : 0u;
+            }
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl[q][c], off);
+                    if (lane >= off) incl[q][c] += y;
+                }
             }
         }
     }
@@ -344,8 +412,9 @@ __device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int 
 }
 
 // Shared memory of hbm_rows_kernel per warp: keys, output rows and stored-compressed flags
-// of its (up to) 32 rows, then two buffers of G row slots.
-constexpr size_t kHbmWarpMetaBytes = 512 + 128;
+// of its (up to) 32 rows, the stream offsets of an all-compressible row (up to 64 words),
+// then two buffers of G row slots.
+constexpr size_t kHbmWarpMetaBytes = 512 + 128 + 256;
 
 template <typename U, int NC, int G>
 __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
@@ -362,12 +431,26 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
     LaneTables<U, NC> lt;
     lt.load(a.s.t, a.s.v);
     const int v = (int)a.s.v, mw = (int)a.s.mw;
+    // stream offsets (inclusive) of a row whose words are all compressible, lane-major
+    uint32_t *full = reinterpret_cast<uint32_t *>(meta + 640);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        uint32_t f = 32 * c + lane < v ? (uint32_t)lt.nb[c] : 0u;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, f, off);
+            if (lane >= off) f += y;
+        }
+        full[c * 32 + lane] = f;
+    }
+    __syncwarp();
     const int nq16 = v / per16;  // 16-byte blocks of a row (<= 32)
     const int64_t nrows = a.list ? (int64_t)*a.list_len : a.nrows;
-    // chunks of 32 rows (double-buffered groups) when every warp gets several of them;
-    // otherwise one group per chunk, so that the rows spread over all warps
+    // chunks of 32 rows (double-buffered groups) when every warp gets several of them, of
+    // 8 (two groups) when every warp gets two, otherwise one group per chunk, so that the
+    // rows spread over all warps (each chunk costs an atomic on the one work counter)
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    const int chunk = nrows >= 4 * 32 * nwarps ? 32 : G;
+    const int chunk = nrows >= 4 * 32 * nwarps ? 32 : (nrows >= 16 * nwarps ? 8 : G);
     const unsigned below = (1u << lane) - 1u;
     for (;;) {
         unsigned long long c0 = 0;
@@ -377,14 +460,17 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
         const int avail = (int)min((int64_t)chunk, nrows - p0);
         const bool valid = lane < avail;
         int64_t k = p0 + lane, key = k;
+        int packed = 0;
         if (valid && a.list) {  // a head record of the claim pass: position and row
             const longlong2 r = reinterpret_cast<const longlong2 *>(a.list)[p0 + lane];
-            k = r.x;
+            k = (int64_t)((uint64_t)r.x & ~kRecordPacked);
             key = r.y;
+            packed = r.x < 0;
         }
         const bool bad = valid && (key < 0 || key >= a.s.n);
         if (bad) atomicOr(a.status, kStatusBadIndex);
         const bool ok = valid && !bad;
+        if (ok && !a.list) packed = (__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1;
         // the chunk's rows, packed to the front of its metadata
         const unsigned fm = __ballot_sync(0xffffffffu, ok);
         const int rows = __popc(fm);
@@ -392,7 +478,7 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
             const int slot = __popc(fm & below);
             mkey[slot] = key;
             mout[slot] = a.out + k * (int64_t)v;
-            mpk[slot] = (__ldg(&a.s.bitmask[key >> 5]) >> (key & 31)) & 1;
+            mpk[slot] = packed;
         }
         __syncwarp();
         const unsigned okm = rows == 32 ? 0xffffffffu : ((1u << rows) - 1u);
@@ -420,7 +506,7 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
             }
             __syncwarp();
             hbm_decode_group<U, NC, G>(bufs + (g & 1) * G * sw, sw, g * G, rows, okm, pm, v, mw,
-                                       lt, mout, a.status);
+                                       lt, full, mout, a.status);
             __syncwarp();
         }
     }
@@ -445,10 +531,8 @@ static ibp_status launch_hbm_nc(FetchArgs<U> a, cudaStream_t st) {
     const size_t smem =
         (size_t)(threads / 32) * (kHbmWarpMetaBytes + 2 * G * a.slot_words * sizeof(U));
     auto kern = hbm_rows_kernel<U, NC, G>;
-    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-    if (per_sm < 1) per_sm = 1;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, threads, smem, &per_sm));
     int64_t blocks = (int64_t)device_sm_count() * per_sm;
     const int64_t need = (a.nrows + (int64_t)G * (threads / 32) - 1) / ((int64_t)G * (threads / 32));
     if (!a.list && blocks > need) blocks = need;
@@ -547,14 +631,9 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     }
     a.slots = slots;
     auto kern = fetch_rows_kernel<U, NC, EXACT, ASYNC>;
-    IBP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int64_t blocks = nblks;
-    if (blocks <= 0) {
-        int per_sm = 0;
-        IBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-        if (per_sm < 1) per_sm = 1;
-        blocks = (int64_t)device_sm_count() * per_sm;
-    }
+    int per_sm = 0;
+    IBP_RET(kernel_blocks_per_sm((const void *)kern, threads, smem, &per_sm));
+    int64_t blocks = nblks > 0 ? nblks : (int64_t)device_sm_count() * per_sm;
     a.upos = unit_positions(a.nrows, blocks * (threads / 32));
     // host rows: a warp takes no more positions than it has row slots, so the rows the
     // whole grid has in flight stay close together in host memory; HBM rows: 32
@@ -603,6 +682,36 @@ static ibp_status launch_fetch(FetchArgs<U> a, int nblks, int nthreads, cudaStre
     return launch_fetch_x<U, false, false>(a, nblks, nthreads, st);
 }
 
+// The first kernel of a fetch call, in place of two memsets and the table build (a per-call
+// fetch of a few thousand rows is as long as a handful of launches): clears the status word
+// and the counters (the first 192 bytes of the workspace), builds the column tables unless
+// the call only gathers raw rows, and marks `fill_pairs` 16-byte entries of the claim table
+// empty (all ones).
+template <typename U>
+__global__ void __launch_bounds__(256)
+prep_fetch_kernel(int32_t *status, const U *__restrict__ mask, const U *__restrict__ bitval,
+                  int64_t v, ColTables<U> t, bool tables, longlong2 *fill, int64_t fill_pairs) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
+    if (tid < 48) status[tid] = 0;
+    if (tables)
+        for (int64_t j = tid; j < v; j += nthr) build_table_column<U>(mask, bitval, v, t, j);
+    for (int64_t i = tid; i < fill_pairs; i += nthr) fill[i] = make_longlong2(-1, -1);
+}
+
+template <typename U>
+static ibp_status launch_prep(int32_t *status, const U *mask, const U *bitval, int64_t v,
+                              const ColTables<U> &t, bool tables, int64_t *fill, int64_t fill_words,
+                              cudaStream_t st) {
+    const int64_t pairs = fill_words / 2;  // claim tables have an even number of words
+    int64_t blocks = std::max<int64_t>(tables ? (v + 255) / 256 : 1, (pairs + 1023) / 1024);
+    blocks = std::min<int64_t>(std::max<int64_t>(blocks, 1), (int64_t)device_sm_count() * 8);
+    prep_fetch_kernel<U><<<(unsigned)blocks, 256, 0, st>>>(
+        status, mask, bitval, v, t, tables, reinterpret_cast<longlong2 *>(fill), pairs);
+    IBP_LAUNCHED("prep_fetch_kernel");
+    return IBP_OK;
+}
+
 template <typename U>
 ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                            const U *bitval, const int32_t *bitmask, const int64_t *idx,
@@ -621,10 +730,12 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     int32_t *status = c.take<int32_t>(kStatusBytes / sizeof(int32_t));
     ColTables<U> t = carve_tables<U>(c, v);
     // status word (offset 0), the fetch work counter (offset 64), the claimed-head count of a
-    // hashed fetch (offset 128)
-    IBP_CUDA(cudaMemsetAsync(status, 0, 192, st));
-    if (nrows <= 0 || v <= 0) return IBP_OK;
-    if (impl != 2) IBP_RET(build_tables<U>(mask, bitval, v, t, st));
+    // hashed fetch (offset 128): cleared by the call's first kernel (prep_fetch_kernel)
+    if (nrows <= 0 || v <= 0) {
+        IBP_CUDA(cudaMemsetAsync(status, 0, 192, st));
+        return IBP_OK;
+    }
+    const bool tables = impl != 2;
 
     bool on_device = false;
     {
@@ -655,9 +766,13 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
     a.out = out;
     a.status = status;
     a.work = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 64);
-    if (!has_index) return launch_fetch<U>(a, nblks, nthreads, st);
+    if (!has_index) {
+        IBP_RET(launch_prep<U>(status, mask, bitval, v, t, tables, nullptr, 0, st));
+        return launch_fetch<U>(a, nblks, nthreads, st);
+    }
 
     if (nidx > 0x7fffffffLL) {
+        IBP_CUDA(cudaMemsetAsync(status, 0, 192, st));
         set_error("decompress_fetch: index arrays above 2^31-1 entries are not supported");
         return IBP_ERR_UNSUPPORTED;
     }
@@ -673,8 +788,11 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
         int64_t *hkeys = c.take<int64_t>(slots);
         int64_t *hpos = c.take<int64_t>(slots);
         int64_t *heads = c.take<int64_t>(2 * nidx);
-        // keys -1 (empty); positions -1 (unpublished) for the in-fetch claims
-        IBP_CUDA(cudaMemsetAsync(hkeys, 0xFF, (char *)(hpos + slots) - (char *)hkeys, st));
+        // keys -1 (empty); positions -1 (unpublished) for the in-fetch claims (a claim pass
+        // writes the position of each slot it claims); hpos follows hkeys directly (slots is
+        // a multiple of 64 words)
+        IBP_RET(launch_prep<U>(status, mask, bitval, v, t, tables, hkeys,
+                               on_device ? slots : (int64_t)(hpos + slots - hkeys), st));
         a.keys = idx;
         if (on_device) {
             // HBM rows: claim in a pass of its own, so the fetch walks distinct rows only, 32
@@ -685,8 +803,8 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
                 std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
             a.list = heads;
             a.list_len = nheads;
-            // the HBM-row kernel reads head records (position, row)
-            const bool records = hbm_rows_fit(a);
+            // the HBM-row kernel reads head records (position and stored-compressed flag, row)
+            const int32_t *records = hbm_rows_fit(a) ? bitmask : nullptr;
             claim_heads_kernel<<<(unsigned)cb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
                                                              heads, nheads, status, records);
             IBP_LAUNCHED("claim_heads_kernel");
@@ -697,12 +815,9 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
             return launch_fetch<U>(a, nblks, nthreads, st);
         }
         IBP_RET(launch_fetch<U>(a, nblks, nthreads, st));
-        const int64_t fb = std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
-        fill_hashed_kernel<U><<<(unsigned)fb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
-                                                            out, v);
-        IBP_LAUNCHED("fill_hashed_kernel");
-        return IBP_OK;
+        return launch_fill_hashed<U>(idx, nidx, n, hkeys, hpos, slots, out, v, st);
     }
+    IBP_RET(launch_prep<U>(status, mask, bitval, v, t, tables, nullptr, 0, st));
     int64_t *iota = c.take<int64_t>(nidx);
     int64_t *keys_in = c.take<int64_t>(nidx);
     int64_t *keys = c.take<int64_t>(nidx);

@@ -706,8 +706,11 @@ __device__ __forceinline__ void store_release(int64_t *p, int64_t x) {
 
 // Copy rows src -> dst for the lanes of `dm` (each lane's src/dst), four rows at a time: all
 // four rows' loads before any store (16-byte moves when the rows are aligned), so the loads'
-// latencies overlap.  Sources are read through L2 (other SMs may have just written them).
-template <typename U>
+// latencies overlap.  Sources are read through L2 (other SMs may have just written them),
+// or, with kCached (sources written by an earlier kernel and not written during this one),
+// through the SM's L1 as well, so that a hot row copied by many warps of an SM is read from
+// L2 once per SM instead of once per copy.
+template <typename U, bool kCached = false>
 __device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_row, int64_t v,
                                           bool vec_rows) {
     constexpr int R = 4;
@@ -736,7 +739,9 @@ __device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_
                 uint4 t[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (r < cnt) t[r] = __ldcg(reinterpret_cast<const uint4 *>(src[r]) + q);
+                    if (r < cnt)
+                        t[r] = kCached ? __ldg(reinterpret_cast<const uint4 *>(src[r]) + q)
+                                       : __ldcg(reinterpret_cast<const uint4 *>(src[r]) + q);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
                     if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
@@ -746,7 +751,7 @@ __device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_
                 U t[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (r < cnt) t[r] = __ldcg(src[r] + q);
+                    if (r < cnt) t[r] = kCached ? __ldg(src[r] + q) : __ldcg(src[r] + q);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
                     if (r < cnt) dst[r][q] = t[r];

@@ -38,6 +38,18 @@ def _stream():
     return torch.cuda.current_stream().cuda_stream
 
 
+# Per-call fast paths (the device index and its current stream as plain integers); the public
+# torch.cuda helpers they stand in for cost microseconds of Python per call.
+_get_device = getattr(torch._C, "_cuda_getDevice", None) or torch.cuda.current_device
+_raw_stream = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
+def _stream_of(index):
+    if _raw_stream is not None:
+        return _raw_stream(index)
+    return torch.cuda.current_stream(index).cuda_stream
+
+
 def _ptr(t):
     return None if t is None else t.data_ptr()
 
@@ -277,15 +289,16 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
     RuntimeError when an index was out of range or a row could not be decoded; the default
     leaves those rows unwritten without a host synchronisation (print_debug(True) prints a
     message instead)."""
-    _torch_check(comp_dataset.device.type == "cuda" or comp_dataset.is_pinned(),
+    _torch_check(comp_dataset.is_cuda or comp_dataset.is_pinned(),
                  "Input tensor must accessible by CUDA device (GPU or pinned memory)")
-    _torch_check(comp_dataset.dim() in (1, 2),
+    dim = comp_dataset.dim()
+    _torch_check(dim in (1, 2),
                  "Input tensor must be 1D [vec_size] or 2D [num_vecs x vec_size] got "
-                 f"{comp_dataset.dim()}")
+                 f"{dim}")
     _torch_check(comp_dataset.is_contiguous(), "Input tensor must be contiguous")
-    _torch_check(_gpu_accessible(mask),
+    _torch_check(mask.is_cuda or mask.is_pinned(),
                  "Mask tensor must accessible by CUDA device (GPU or pinned memory)")
-    _torch_check(_gpu_accessible(bitval),
+    _torch_check(bitval.is_cuda or bitval.is_pinned(),
                  "Bitval tensor must accessible by CUDA device (GPU or pinned memory)")
     wb = comp_dataset.element_size()
     _torch_check(wb in (4, 8), "Input tensor must be 4-byte or 8-byte datatype")
@@ -294,17 +307,22 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
                  "as input dataset")
     if bitmask.dtype != torch.int32:
         raise RuntimeError(f"expected scalar type Int but found {bitmask.dtype}")
-    n = 1 if comp_dataset.dim() == 1 else comp_dataset.shape[0]
-    v = comp_dataset.shape[0] if comp_dataset.dim() == 1 else comp_dataset.shape[1]
-    out_device = torch.device(out_device)
+    shape = comp_dataset.shape
+    n, v = (1, shape[0]) if dim == 1 else (shape[0], shape[1])
+    if not isinstance(out_device, torch.device):
+        out_device = torch.device(out_device)
     if out_device.type == "cuda" and out_device.index is None:
-        out_device = torch.device("cuda", torch.cuda.current_device())
+        out_device = torch.device("cuda", _get_device())
     idx = None
     if index_array_ is not None:
-        _torch_check(index_array_.device.type == "cuda",
+        _torch_check(index_array_.is_cuda,
                      "Index array must accessible by CUDA device (GPU or pinned memory)")
         _torch_check(index_array_.dim() == 1, "Index array should be 1D")
-        idx = index_array_.to(torch.int64).contiguous()
+        idx = index_array_
+        if idx.dtype != torch.int64:
+            idx = idx.to(torch.int64)
+        if not idx.is_contiguous():
+            idx = idx.contiguous()
     nrows = n if idx is None else idx.shape[0]
     impl = -1 if impl_ is None else int(impl_)
     comp_len = v
@@ -324,22 +342,35 @@ def decompress_fetch(comp_dataset, mask, bitval, bitmask, out_device, comp_len_=
     if out_device.type != "cuda" and not out.is_pinned():
         out = out.pin_memory()
     dev = _cuda_device(comp_dataset, mask, idx, out)
-    with torch.cuda.device(dev):
-        need = _lib.ibp_decompress_fetch_workspace_size(nrows, v, wb, 0 if idx is None else 1)
-        ws, wsb = _workspace(need, dev)
-        _check(_lib.ibp_decompress_fetch(
-            _ptr(comp_dataset), n, v, wb, _ptr(mask), _ptr(bitval), _ptr(bitmask), _ptr(idx),
-            -1 if idx is None else nrows, comp_len, _ptr(out),
-            -1 if nblks_ is None else int(nblks_),
-            -1 if nthreads_ is None else int(nthreads_), impl, _ptr(ws), wsb, _stream()))
-        if check:
-            _raise_on_status(ws, "decompress_fetch")
-        elif _debug and ws is not None:
-            st = torch.zeros(1, dtype=torch.int32)
-            import ctypes
-            _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), _stream()))
-            if int(st[0]) & 1:
-                print("[ibp] decompress_fetch: an index was out of range; its rows were skipped")
+    cur = _get_device()
+    if dev.index is not None and dev.index != cur:
+        with torch.cuda.device(dev):
+            return _fetch_call(comp_dataset, n, v, wb, mask, bitval, bitmask, idx, nrows,
+                               comp_len, out, nblks_, nthreads_, impl, dev, dev.index, check)
+    return _fetch_call(comp_dataset, n, v, wb, mask, bitval, bitmask, idx, nrows, comp_len,
+                       out, nblks_, nthreads_, impl, dev, cur, check)
+
+
+def _fetch_call(comp_dataset, n, v, wb, mask, bitval, bitmask, idx, nrows, comp_len, out,
+                nblks_, nthreads_, impl, dev, dev_index, check):
+    need = _lib.ibp_decompress_fetch_workspace_size(nrows, v, wb, 0 if idx is None else 1)
+    ws, wsb = _workspace(need, dev)
+    stream = _stream_of(dev_index)
+    _check(_lib.ibp_decompress_fetch(
+        comp_dataset.data_ptr(), n, v, wb, mask.data_ptr(), bitval.data_ptr(),
+        bitmask.data_ptr(), None if idx is None else idx.data_ptr(),
+        -1 if idx is None else nrows, comp_len, out.data_ptr(),
+        -1 if nblks_ is None else int(nblks_),
+        -1 if nthreads_ is None else int(nthreads_), impl,
+        None if ws is None else ws.data_ptr(), wsb, stream))
+    if check:
+        _raise_on_status(ws, "decompress_fetch")
+    elif _debug and ws is not None:
+        st = torch.zeros(1, dtype=torch.int32)
+        import ctypes
+        _check(_lib.ibp_read_status(_ptr(ws), ctypes.c_void_p(st.data_ptr()), stream))
+        if int(st[0]) & 1:
+            print("[ibp] decompress_fetch: an index was out of range; its rows were skipped")
     return out
 
 
