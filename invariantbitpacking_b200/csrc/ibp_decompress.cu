@@ -296,31 +296,26 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
 // words whole) takes its stream offsets from a table made once per warp; otherwise its prefix
 // sums are issued together.  The row's stream length falls out of the offsets (no separate
 // length pass, no tail reads), and stream offsets are 32-bit.
+//
+// Stream reads: 32-bit units of the MSB-first stream with two funnel shifts (stream unit t is
+// memory unit t ^ 1 for 64-bit words, whose high half comes second in memory, and unit t for
+// 32-bit words).  A word is read as the W stream bits that end where its bits end,
+// right-aligned: a compressible word's L kept bits come out in the low bits with whatever
+// precedes them above, and its scatter never moves those upper bits to a kept position (each
+// kept position takes exactly one of the low L bits), so they need no masking, and neither
+// the kept-bit count nor a variable shift enters the read.  For e < W the window starts
+// before the stream, in the row's last bitmap word, which the row buffer holds.
 template <typename U>
-__device__ __forceinline__ U stream_bits(const U *words, uint32_t s, int L) {
-    constexpr int W = 8 * sizeof(U);
-    const uint32_t q = s / W;
-    const int r = (int)(s % W);
-    const U hi = words[q], lo = words[q + 1];
-    // (lo >> 1) >> (W - 1 - r) is lo >> (W - r) for r >= 1 and 0 for r == 0
-    const U win = (U)((hi << r) | ((lo >> 1) >> (W - 1 - r)));
-    return L == 0 ? (U)0 : (U)(win >> (W - L));
-}
-
-// The same read from 32-bit units of the MSB-first stream with two funnel shifts: stream unit
-// t is memory unit t ^ 1 for 64-bit words (the high half of a little-endian word comes
-// second) and unit t for 32-bit words.  Reads the same words as stream_bits.
-template <typename U>
-__device__ __forceinline__ U stream_bits_funnel(const U *words, uint32_t s, int L) {
+__device__ __forceinline__ U stream_bits_ending(const U *words, int32_t e) {
     const uint32_t *u = reinterpret_cast<const uint32_t *>(words);
-    const uint32_t t = s >> 5, r = s & 31;
+    const int32_t s = e - 8 * (int32_t)sizeof(U);
+    const int32_t t = s >> 5;  // may be -2 or -1 (the bitmap's last word)
+    const uint32_t r = (uint32_t)s & 31u;
     if constexpr (sizeof(U) == 8) {
         const uint32_t a = u[t ^ 1], b = u[(t + 1) ^ 1], c = u[(t + 2) ^ 1];
-        const uint64_t win = ((uint64_t)__funnelshift_l(b, a, r) << 32) | __funnelshift_l(c, b, r);
-        return L == 0 ? (U)0 : (U)(win >> (64 - L));
+        return ((uint64_t)__funnelshift_l(b, a, r) << 32) | __funnelshift_l(c, b, r);
     } else {
-        const uint32_t win = __funnelshift_l(u[t + 1], u[t], r);
-        return L == 0 ? (U)0 : (U)(win >> (32 - L));
+        return __funnelshift_l(u[t + 1], u[t], r);
     }
 }
 
@@ -402,9 +397,7 @@ __device__ __forceinline__ void hbm_decode_group(const U *__restrict__ buf, int 
             const int j = 32 * c + lane;
             if (j < v) {
                 const bool cj = (cjm >> (q * NC + c)) & 1u;
-                const int L = cj ? (int)lt.nb[c] : W;
-                const U y =
-                    stream_bits_funnel<U>(stream, (c ? t0 : 0u) + incl[q][c] - (uint32_t)L, L);
+                const U y = stream_bits_ending<U>(stream, (int32_t)((c ? t0 : 0u) + incl[q][c]));
                 o[j] = cj ? (U)(lt.bv[c] | scatter_regs<U>(y, (U)~lt.m[c], lt.mv[c])) : y;
             }
         }
