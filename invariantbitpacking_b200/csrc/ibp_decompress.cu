@@ -74,10 +74,13 @@ constexpr uint64_t kRecordPacked = 1ull << 63;  // head record: the row is store
 // Claim pass of a hashed fetch: every position claims its row; the positions that win are
 // appended to `heads` (one atomic per block and pass, so the list's counter is not a hot
 // spot), and the fetch kernel then walks distinct rows only, 32 to a chunk.  Out-of-range
-// rows are flagged here and never claimed.  256 threads per block, one position each.
+// rows are flagged here and never claimed.  256 threads per block, P positions each.
 // bitmask != nullptr: each listed head is a record of two words, its position (bit 63 set
 // when the row is stored compressed) and its row, so that a fetch reads one 16-byte record
 // per row instead of a position, then the index entry it points to, then the bitmask word.
+// P positions per thread and pass: 2 when one position per thread would need more than one
+// wave of resident blocks (fewer block-wide rounds), else 1 (more blocks for small batches).
+template <int P>
 __global__ void __launch_bounds__(256)
 claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int64_t *hkeys,
                    int64_t *hpos, int64_t hslots, int64_t *__restrict__ heads,
@@ -86,44 +89,62 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
     const bool records = bitmask != nullptr;
     __shared__ unsigned counts[8];
     __shared__ unsigned long long block_base;
-    // the block's own table of the rows its 256 positions hold (empty: ~0), so that a hot row
-    // of a skewed batch is claimed once per block: every claim of one row reads the same
+    // the block's own table of the rows its 256 x P positions hold (empty: ~0), so that a hot
+    // row of a skewed batch is claimed once per block: every claim of one row reads the same
     // global slot, which one L2 slice serves
-    constexpr int kBlockSlots = 512;
+    constexpr int kBlockSlots = 512 * P;
     __shared__ unsigned long long btab[kBlockSlots];
     for (int i = threadIdx.x; i < kBlockSlots; i += 256) btab[i] = ~0ull;
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int64_t b0 = (int64_t)blockIdx.x * 256; b0 < nidx; b0 += (int64_t)gridDim.x * 256) {
-        const int64_t k = b0 + threadIdx.x;
-        const int64_t key = k < nidx ? idx[k] : 0;
-        const bool bad = k < nidx && (key < 0 || key >= n);
-        if (bad) atomicOr(status, kStatusBadIndex);
-        const bool ok = k < nidx && !bad;
-        // the row's bitmask word, loaded before the claim so that the two latencies overlap
-        const int32_t bmw = records && ok ? __ldg(&bitmask[key >> 5]) : 0;
-        // one claim per distinct row of the warp (the lowest lane holding it)
-        const unsigned same = __match_any_sync(0xffffffffu, ok ? key : (int64_t)-1);
-        bool lead = ok && (__ffs(same) - 1) == lane;
-        if (lead) {
-            uint32_t h = (uint32_t)row_hash(key, kBlockSlots);
-            for (int probe = 0; probe < kBlockSlots; ++probe) {
-                const unsigned long long old = atomicCAS(&btab[h], ~0ull, (unsigned long long)key);
-                if (old == ~0ull) break;  // the block's first position of this row
-                if (old == (unsigned long long)key) {
-                    lead = false;
-                    break;
+    const unsigned below = (1u << lane) - 1u;
+    for (int64_t b0 = (int64_t)blockIdx.x * 256 * P; b0 < nidx;
+         b0 += (int64_t)gridDim.x * 256 * P) {
+        int64_t k[P], key[P];
+        bool ok[P], head[P];
+        int32_t bmw[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            k[p] = b0 + p * 256 + threadIdx.x;
+            key[p] = k[p] < nidx ? idx[k[p]] : 0;
+            const bool bad = k[p] < nidx && (key[p] < 0 || key[p] >= n);
+            if (bad) atomicOr(status, kStatusBadIndex);
+            ok[p] = k[p] < nidx && !bad;
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            // the row's bitmask word, loaded before the claim so that the latencies overlap
+            bmw[p] = records && ok[p] ? __ldg(&bitmask[key[p] >> 5]) : 0;
+        }
+        unsigned hm[P];
+        unsigned total = 0;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            // one claim per distinct row of the warp (the lowest lane holding it)
+            const unsigned same = __match_any_sync(0xffffffffu, ok[p] ? key[p] : (int64_t)-1);
+            bool lead = ok[p] && (__ffs(same) - 1) == lane;
+            if (lead) {
+                uint32_t h = (uint32_t)row_hash(key[p], kBlockSlots);
+                for (int probe = 0; probe < kBlockSlots; ++probe) {
+                    const unsigned long long old =
+                        atomicCAS(&btab[h], ~0ull, (unsigned long long)key[p]);
+                    if (old == ~0ull) break;  // the block's first position of this row
+                    if (old == (unsigned long long)key[p]) {
+                        lead = false;
+                        break;
+                    }
+                    h = (h + 1) & (kBlockSlots - 1);
                 }
-                h = (h + 1) & (kBlockSlots - 1);
             }
+            head[p] = false;
+            if (lead) {
+                const int64_t slot = hash_claim_slot(hkeys, hslots, key[p], head[p]);
+                if (head[p]) hpos[slot] = k[p];
+            }
+            hm[p] = __ballot_sync(0xffffffffu, head[p]);
+            total += __popc(hm[p]);
         }
-        bool head = false;
-        if (lead) {
-            const int64_t slot = hash_claim_slot(hkeys, hslots, key, head);
-            if (head) hpos[slot] = k;
-        }
-        const unsigned hm = __ballot_sync(0xffffffffu, head);
-        if (lane == 0) counts[wid] = __popc(hm);
+        if (lane == 0) counts[wid] = total;
         __syncthreads();
         if (threadIdx.x == 0) {
             unsigned run = 0;
@@ -135,12 +156,17 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
             block_base = run ? atomicAdd(nheads, (unsigned long long)run) : 0ull;
         }
         __syncthreads();
-        const unsigned long long at = block_base + counts[wid] + __popc(hm & ((1u << lane) - 1u));
-        if (head && !records) heads[at] = k;
-        if (head && records) {
-            const bool packed = (bmw >> (key & 31)) & 1;
-            reinterpret_cast<longlong2 *>(heads)[at] =
-                make_longlong2(packed ? (int64_t)((uint64_t)k | kRecordPacked) : k, key);
+        unsigned long long at = block_base + counts[wid];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const unsigned long long my = at + __popc(hm[p] & below);
+            if (head[p] && !records) heads[my] = k[p];
+            if (head[p] && records) {
+                const bool packed = (bmw[p] >> (key[p] & 31)) & 1;
+                reinterpret_cast<longlong2 *>(heads)[my] = make_longlong2(
+                    packed ? (int64_t)((uint64_t)k[p] | kRecordPacked) : k[p], key[p]);
+            }
+            at += __popc(hm[p]);
         }
         for (int i = threadIdx.x; i < kBlockSlots; i += 256) btab[i] = ~0ull;
         __syncthreads();  // counts, block_base and btab are rewritten by the next pass
@@ -792,14 +818,20 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
             // to a chunk (the fetch is latency-bound here and chunks of repeats cost it)
             auto *nheads =
                 reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(status) + 128);
-            const int64_t cb =
-                std::min<int64_t>((nidx + 255) / 256, (int64_t)device_sm_count() * 8);
+            const int64_t wave = (int64_t)device_sm_count() * 8;  // resident 256-thread blocks
+            const bool two = nidx > 256 * wave;
+            const int64_t cb = std::min<int64_t>((nidx + (two ? 511 : 255)) / (two ? 512 : 256),
+                                                 wave);
             a.list = heads;
             a.list_len = nheads;
             // the HBM-row kernel reads head records (position and stored-compressed flag, row)
             const int32_t *records = hbm_rows_fit(a) ? bitmask : nullptr;
-            claim_heads_kernel<<<(unsigned)cb, 256, 0, st>>>(idx, nidx, n, hkeys, hpos, slots,
-                                                             heads, nheads, status, records);
+            if (two)
+                claim_heads_kernel<2><<<(unsigned)cb, 256, 0, st>>>(
+                    idx, nidx, n, hkeys, hpos, slots, heads, nheads, status, records);
+            else
+                claim_heads_kernel<1><<<(unsigned)cb, 256, 0, st>>>(
+                    idx, nidx, n, hkeys, hpos, slots, heads, nheads, status, records);
             IBP_LAUNCHED("claim_heads_kernel");
         } else {
             // host rows: claims and repeat copies happen inside the fetch, hidden behind its
