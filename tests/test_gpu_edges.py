@@ -303,6 +303,34 @@ def test_device_rows_up_to_64_words(ibp, oracle, wb, v, mode):
         _capi.check(_capi.lib.ibp_set_fetch_dedup(0))
 
 
+@pytest.mark.parametrize("wb", [4, 8])
+def test_device_rows_large_batches(ibp, oracle, wb):
+    """Device-resident batches larger than one wave of claim-pass blocks (two positions per
+    thread there; 8-row chunks in the HBM-row kernel), Zipf-skewed and uniform: most rows have
+    every word compressible (the fixed-offset decode), a fifth have some words stored whole
+    (the prefix-sum decode), a few are stored raw; all exact, with the repeat copies."""
+    from invariantbitpacking_b200 import synthetic
+    rng = np.random.default_rng(3000 + wb)
+    n, v = 150_000, 64
+    d, m, b = masked_rows(rng, n, v, wb, frac=0.7, flip=0.0)
+    ut = {4: np.uint32, 8: np.uint64}[wb]
+    mixed = rng.choice(n, n // 5, replace=False)
+    words = rng.integers(0, v, (mixed.size, 3))
+    noise = rng.integers(0, 2**63, (mixed.size, 3), dtype=np.uint64).astype(ut).view(d.dtype)
+    d[mixed[:, None], words] = noise
+    raw = rng.choice(n, n // 50, replace=False)
+    d[raw] = rng.integers(0, 2**63, (raw.size, v), dtype=np.uint64).astype(ut).view(d.dtype)
+    dm, db = torch.from_numpy(m).cuda(), torch.from_numpy(b).cuda()
+    x = torch.from_numpy(d.copy()).pin_memory()
+    bm = ibp.compress_inplace(x, dm, db)
+    xd = x.cuda()
+    z = synthetic.Zipf(n, 1.1, seed=31)
+    for idx in (z.sample(400_000), rng.integers(0, n, 320_000).astype(np.int64)):
+        out = ibp.decompress_fetch(xd, dm, db, bm, "cuda", None, torch.from_numpy(idx).cuda(),
+                                   check=True)
+        assert same(npy(out), d[idx])
+
+
 @pytest.mark.parametrize("where", ["host", "device"])
 @pytest.mark.parametrize("wb,v", [(8, 64), (4, 64), (8, 24), (8, 200)])
 def test_corrupt_rows_are_flagged_and_skipped(ibp, oracle, where, wb, v):
