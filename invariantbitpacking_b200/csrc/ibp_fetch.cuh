@@ -709,7 +709,9 @@ __device__ __forceinline__ void store_release(int64_t *p, int64_t x) {
 // latencies overlap.  Sources are read through L2 (other SMs may have just written them),
 // or, with kCached (sources written by an earlier kernel and not written during this one),
 // through the SM's L1 as well, so that a hot row copied by many warps of an SM is read from
-// L2 once per SM instead of once per copy.
+// L2 once per SM instead of once per copy; the copies are then written as streaming stores
+// (evicted from L2 first), which keeps the sources in L2 (fill of a 400k-row batch's
+// repeats: 39.0 -> 36.5 us).
 template <typename U, bool kCached = false>
 __device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_row, int64_t v,
                                           bool vec_rows) {
@@ -744,7 +746,12 @@ __device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_
                                        : __ldcg(reinterpret_cast<const uint4 *>(src[r]) + q);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (r < cnt) reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
+                    if (r < cnt) {
+                        if (kCached)
+                            __stcs(reinterpret_cast<uint4 *>(dst[r]) + q, t[r]);
+                        else
+                            reinterpret_cast<uint4 *>(dst[r])[q] = t[r];
+                    }
             }
         } else {
             for (int64_t q = lane; q < v; q += 32) {
@@ -754,7 +761,12 @@ __device__ __forceinline__ void copy_rows(unsigned dm, const U *src_row, U *dst_
                     if (r < cnt) t[r] = kCached ? __ldg(src[r] + q) : __ldcg(src[r] + q);
 #pragma unroll
                 for (int r = 0; r < R; ++r)
-                    if (r < cnt) dst[r][q] = t[r];
+                    if (r < cnt) {
+                        if (kCached)
+                            __stcs(dst[r] + q, t[r]);
+                        else
+                            dst[r][q] = t[r];
+                    }
             }
         }
     }
