@@ -18,7 +18,7 @@ has no exchange step); time is the max over ranks.
 The default line also carries the other named configurations, each measured in the same
 run: `plain_small` (16384 x 128 int64, 2048-row fetches: microseconds per call),
 `served_mix` (the continuous-batching server against per-request fetches, ours and the
-reference's, p50/p99 and GB/s at two arrival rates), `embedding_tables` and `decoder_layer`
+reference's, p50/p99 and GB/s at three arrival rates), `embedding_tables` and `decoder_layer`
 (batched multi-set fetches), and `value_1000_steps` (the headline over a long region).
 `--no-extras` leaves them out.
 
