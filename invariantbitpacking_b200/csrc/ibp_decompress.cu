@@ -471,10 +471,18 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
     const int chunk = nrows >= 4 * 32 * nwarps ? 32 : (nrows >= 16 * nwarps ? 8 : G);
     const unsigned below = (1u << lane) - 1u;
-    for (;;) {
-        unsigned long long c0 = 0;
-        if (lane == 0) c0 = atomicAdd(a.work, (unsigned long long)chunk);
-        const int64_t p0 = (int64_t)__shfl_sync(0xffffffffu, c0, 0);
+    // a warp's first chunk is its own (warp w takes chunk w); later ones come from the work
+    // counter, so the grid's warps do not all queue on the counter at the start
+    const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    for (bool first = true;; first = false) {
+        int64_t p0;
+        if (first) {
+            p0 = gwarp * chunk;
+        } else {
+            unsigned long long c0 = 0;
+            if (lane == 0) c0 = atomicAdd(a.work, (unsigned long long)chunk);
+            p0 = (int64_t)__shfl_sync(0xffffffffu, c0, 0) + nwarps * chunk;
+        }
         if (p0 >= nrows) break;
         const int avail = (int)min((int64_t)chunk, nrows - p0);
         const bool valid = lane < avail;
