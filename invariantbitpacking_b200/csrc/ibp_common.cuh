@@ -106,6 +106,33 @@ struct Sizer {
     size_t total() const { return align_up(used, kAlign); }
 };
 
+// Programmatic dependent launch.  A kernel launched by launch_dependent() may start while the
+// kernel before it on the stream is still running: it may read only inputs of the call and
+// its own shared memory until grid_dep_wait() returns, which happens once that kernel has
+// completed and its writes are visible (at once for a kernel launched normally).
+// grid_dep_release() lets the next such kernel start; a kernel calls it after its own wait,
+// so that the kernel after it never starts before the one before it has completed.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_release() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kern)(KArgs...), unsigned grid, unsigned block,
+                                    size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 int device_sm_count();        // SMs of the current device (cached per device)
 int device_max_smem_optin();  // opt-in shared memory per block (cached per device)
 // Resident blocks per SM (at least 1) of a kernel launched with `threads` and `smem` bytes of

@@ -107,6 +107,12 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
         for (int p = 0; p < P; ++p) {
             k[p] = b0 + p * 256 + threadIdx.x;
             key[p] = k[p] < nidx ? idx[k[p]] : 0;
+        }
+        // the table and status words are cleared by the kernel before this one
+        grid_dep_wait();
+        grid_dep_release();
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
             const bool bad = k[p] < nidx && (key[p] < 0 || key[p] >= n);
             if (bad) atomicOr(status, kStatusBadIndex);
             ok[p] = k[p] < nidx && !bad;
@@ -210,6 +216,8 @@ fill_hashed_kernel(const int64_t *__restrict__ idx, int64_t nrows, int64_t n,
         int64_t hp = -1;
         if (key >= 0 && key < n) hp = hash_find(hkeys, hpos, hslots, key);
         const bool rep = hp >= 0 && hp != k;
+        // the first occurrences' rows are written by the kernel before this one
+        grid_dep_wait();
         copy_rows<U, true>(__ballot_sync(0xffffffffu, rep), out + (rep ? hp : 0) * v,
                            out + (rep ? k : 0) * v, v, vec_rows);
     }
@@ -225,7 +233,8 @@ static ibp_status launch_fill_hashed(const int64_t *idx, int64_t nidx, int64_t n
     IBP_RET(kernel_blocks_per_sm((const void *)kern, kFillThreads, 0, &per_sm));
     const int64_t fb = std::min<int64_t>((nidx + kFillThreads - 1) / kFillThreads,
                                          (int64_t)device_sm_count() * per_sm);
-    kern<<<(unsigned)fb, kFillThreads, 0, st>>>(idx, nidx, n, hkeys, hpos, slots, out, v);
+    IBP_CUDA(launch_dependent(kern, (unsigned)fb, kFillThreads, 0, st, idx, nidx, n, hkeys, hpos,
+                              slots, out, v));
     IBP_LAUNCHED("fill_hashed_kernel");
     return IBP_OK;
 }
@@ -237,6 +246,8 @@ static ibp_status launch_fill_hashed(const int64_t *idx, int64_t nidx, int64_t n
 template <typename U, int NC, bool EXACT, bool ASYNC>
 __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<U> a) {
     extern __shared__ __align__(16) unsigned char smem[];
+    // tables, counters, claim table and sorted keys come from the kernels before this one
+    grid_dep_wait();
     constexpr bool kClaims = !ASYNC;  // in-fetch claims: host rows (fixed-stride or condensed)
     const int lane = threadIdx.x & 31;
     U *slots = reinterpret_cast<U *>(smem) +
@@ -447,6 +458,10 @@ __global__ void __launch_bounds__(256, 4) hbm_rows_kernel(FetchArgs<U> a) {
     const int sw = (int)a.slot_words;
     U *bufs = reinterpret_cast<U *>(smem + (blockDim.x >> 5) * kHbmWarpMetaBytes) +
               (int64_t)warp * 2 * G * sw;
+    // the column tables, the claim pass's list, the work counter and the status words come
+    // from the kernels before this one
+    grid_dep_wait();
+    grid_dep_release();
     LaneTables<U, NC> lt;
     lt.load(a.s.t, a.s.v);
     const int v = (int)a.s.v, mw = (int)a.s.mw;
@@ -564,7 +579,7 @@ static ibp_status launch_hbm_nc(FetchArgs<U> a, cudaStream_t st) {
     const int64_t need = (a.nrows + (int64_t)G * (threads / 32) - 1) / ((int64_t)G * (threads / 32));
     if (!a.list && blocks > need) blocks = need;
     const int slot = profile_begin(st);
-    kern<<<(unsigned)blocks, threads, smem, st>>>(a);
+    IBP_CUDA(launch_dependent(kern, (unsigned)blocks, threads, smem, st, a));
     IBP_LAUNCHED("hbm_rows_kernel");
     profile_end(slot, st);
     return IBP_OK;
@@ -669,7 +684,7 @@ static ibp_status launch_fetch_nc(FetchArgs<U> a, int nblks, int nthreads, cudaS
     const int64_t need = (chunks + threads / 32 - 1) / (threads / 32);
     if (blocks > need) blocks = need;
     const int slot = profile_begin(st);
-    kern<<<(unsigned)blocks, threads, smem, st>>>(a);
+    IBP_CUDA(launch_dependent(kern, (unsigned)blocks, threads, smem, st, a));
     IBP_LAUNCHED("fetch_rows_kernel");
     profile_end(slot, st);
     return IBP_OK;
@@ -718,6 +733,7 @@ template <typename U>
 __global__ void __launch_bounds__(256)
 prep_fetch_kernel(int32_t *status, const U *__restrict__ mask, const U *__restrict__ bitval,
                   int64_t v, ColTables<U> t, bool tables, longlong2 *fill, int64_t fill_pairs) {
+    grid_dep_release();  // the claim pass may load its positions meanwhile
     const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t nthr = (int64_t)gridDim.x * blockDim.x;
     if (tid < 48) status[tid] = 0;
@@ -834,12 +850,9 @@ ibp_status decompress_impl(const U *comp, int64_t n, int64_t v, const U *mask,
             a.list_len = nheads;
             // the HBM-row kernel reads head records (position and stored-compressed flag, row)
             const int32_t *records = hbm_rows_fit(a) ? bitmask : nullptr;
-            if (two)
-                claim_heads_kernel<2><<<(unsigned)cb, 256, 0, st>>>(
-                    idx, nidx, n, hkeys, hpos, slots, heads, nheads, status, records);
-            else
-                claim_heads_kernel<1><<<(unsigned)cb, 256, 0, st>>>(
-                    idx, nidx, n, hkeys, hpos, slots, heads, nheads, status, records);
+            IBP_CUDA(launch_dependent(two ? claim_heads_kernel<2> : claim_heads_kernel<1>,
+                                      (unsigned)cb, 256, 0, st, idx, nidx, n, hkeys, hpos, slots,
+                                      heads, nheads, status, records));
             IBP_LAUNCHED("claim_heads_kernel");
         } else {
             // host rows: claims and repeat copies happen inside the fetch, hidden behind its
