@@ -184,8 +184,8 @@ claim_heads_kernel(const int64_t *__restrict__ idx, int64_t nidx, int64_t n, int
 // a time per warp).  The rows it copies were written by the fetch kernel before it, so they
 // are read through L1: the hot rows of a skewed batch then leave L2 once per SM rather than
 // once per copy (one L2 slice holds each 128-byte line of a row, and a Zipf(1.1) batch of
-// 400k positions copies its hottest row ~40k times); the claim table, written by the claim
-// pass, is read the same way.
+// 400k positions over 2.4M rows copies its hottest row ~48k times); the claim table,
+// written by the claim pass, is read the same way.
 constexpr int kFillThreads = 256;
 
 __device__ __forceinline__ int64_t hash_find(const int64_t *__restrict__ keys,
