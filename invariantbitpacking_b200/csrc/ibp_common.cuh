@@ -130,7 +130,14 @@ inline cudaError_t launch_dependent(void (*kern)(KArgs...), unsigned grid, unsig
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    if (e == cudaErrorNotSupported) {
+        // no programmatic launches here: an ordinary launch (the waits then return at once)
+        (void)cudaGetLastError();
+        cfg.numAttrs = 0;
+        e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    }
+    return e;
 }
 
 int device_sm_count();        // SMs of the current device (cached per device)
