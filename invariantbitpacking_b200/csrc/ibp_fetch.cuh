@@ -413,7 +413,9 @@ __device__ __forceinline__ void finish_rows(const RowSet<U> &s, const LaneTables
 // their PCIe or HBM round trips overlap; rows that are not 16-byte aligned, whose first
 // read exceeds 1 KiB or whose tail exceeds 512 bytes take a plain loop.
 // `orow` is each lane's output row.
-template <typename U, int NC>
+// kRawStage: rows stored raw may be staged with the first reads (see below); instantiated
+// false where no raw row can be (rows over 1 KiB), which frees the registers it takes.
+template <typename U, int NC, bool kRawStage = true>
 __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables<U, NC> &lt,
                                             U *__restrict__ slots, int nslots,
                                             int64_t slot_words, int64_t key, U *orow,
@@ -425,8 +427,8 @@ __device__ __forceinline__ void fetch_heads(const RowSet<U> &s, const LaneTables
     // reads when they fit it and the register staging, so copying them out costs no round
     // trip of its own
     const int64_t nq_raw = v / per16;
-    const bool raw_staged = (v % per16) == 0 && v + 2 <= slot_words && nq_raw <= 64 &&
-                            (((uintptr_t)s.comp) & 15) == 0;
+    const bool raw_staged = kRawStage && (v % per16) == 0 && v + 2 <= slot_words &&
+                            nq_raw <= 64 && (((uintptr_t)s.comp) & 15) == 0;
     unsigned hm = __ballot_sync(0xffffffffu, head);
     while (hm) {
         int lid[kRowsInFlight];
