@@ -171,6 +171,29 @@ __device__ __forceinline__ U get_bits(const U *words, int64_t s, int L) {
     return shr_w<U>(win, W - L);
 }
 
+// The W stream bits that end at stream bit e (e >= 1) of `words`, right-aligned: the word
+// whose bits end there, with whatever precedes them above.  Read from 32-bit units with two
+// funnel shifts (stream unit t is memory unit t ^ 1 for 64-bit words, whose high half comes
+// second in memory, and unit t for 32-bit words).  A compressible word's L kept bits come out
+// in the low bits; its scatter never moves the bits above them to a kept position (each kept
+// position takes exactly one of the low L bits), so they need no masking, and neither the
+// kept-bit count nor a variable shift enters the read.  For e < W the window starts before
+// `words`, in the W bits before it, which the caller's buffer holds (a row's bitmap, or the
+// stream's earlier words).
+template <typename U>
+__device__ __forceinline__ U stream_bits_ending(const U *words, int32_t e) {
+    const uint32_t *u = reinterpret_cast<const uint32_t *>(words);
+    const int32_t s = e - 8 * (int32_t)sizeof(U);
+    const int32_t t = s >> 5;  // may be -2 or -1
+    const uint32_t r = (uint32_t)s & 31u;
+    if constexpr (sizeof(U) == 8) {
+        const uint32_t a = u[t ^ 1], b = u[(t + 1) ^ 1], c = u[(t + 2) ^ 1];
+        return ((uint64_t)__funnelshift_l(b, a, r) << 32) | __funnelshift_l(c, b, r);
+    } else {
+        return __funnelshift_l(u[t + 1], u[t], r);
+    }
+}
+
 // Copy `words` W-bit words between global buffers with a warp; 16-byte accesses when both
 // sides are 16-byte aligned.
 template <typename U>

@@ -335,28 +335,8 @@ __global__ void __launch_bounds__(kFetchThreads, 2) fetch_rows_kernel(FetchArgs<
 // sums are issued together.  The row's stream length falls out of the offsets (no separate
 // length pass, no tail reads), and stream offsets are 32-bit.
 //
-// Stream reads: 32-bit units of the MSB-first stream with two funnel shifts (stream unit t is
-// memory unit t ^ 1 for 64-bit words, whose high half comes second in memory, and unit t for
-// 32-bit words).  A word is read as the W stream bits that end where its bits end,
-// right-aligned: a compressible word's L kept bits come out in the low bits with whatever
-// precedes them above, and its scatter never moves those upper bits to a kept position (each
-// kept position takes exactly one of the low L bits), so they need no masking, and neither
-// the kept-bit count nor a variable shift enters the read.  For e < W the window starts
-// before the stream, in the row's last bitmap word, which the row buffer holds.
-template <typename U>
-__device__ __forceinline__ U stream_bits_ending(const U *words, int32_t e) {
-    const uint32_t *u = reinterpret_cast<const uint32_t *>(words);
-    const int32_t s = e - 8 * (int32_t)sizeof(U);
-    const int32_t t = s >> 5;  // may be -2 or -1 (the bitmap's last word)
-    const uint32_t r = (uint32_t)s & 31u;
-    if constexpr (sizeof(U) == 8) {
-        const uint32_t a = u[t ^ 1], b = u[(t + 1) ^ 1], c = u[(t + 2) ^ 1];
-        return ((uint64_t)__funnelshift_l(b, a, r) << 32) | __funnelshift_l(c, b, r);
-    } else {
-        return __funnelshift_l(u[t + 1], u[t], r);
-    }
-}
-
+// Stream reads: stream_bits_ending (ibp_codec.cuh), a word read as the W stream bits that end
+// where its bits end.
 // `full[32 * c + lane]`: the inclusive prefix over the lanes of chunk c of the kept bits of
 // every column (the stream offsets of a row whose words are all compressible).
 template <typename U, int NC, int G>

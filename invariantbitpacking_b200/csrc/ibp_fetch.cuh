@@ -123,13 +123,16 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
             base += __shfl_sync(0xffffffffu, incl, 31);
         }
     } else {
+        // four chunks of 32 columns at a time; bit offsets relative to the stream word that
+        // holds the group's first bit, so they stay 32-bit however long the row
         constexpr int G = 4;
-        int64_t base = 0;
+        constexpr int LW = LogW<U>::value;
+        int64_t base = 0;  // stream bits of the row's earlier groups
         for (int64_t g0 = 0; g0 < v; g0 += 32 * G) {
             U m[G], bv[G];
             bool in[G], cj[G];
-            int len[G], incl[G];
-            bool few = true;  // every column of the group keeps at most 4 bits
+            int incl[G];
+            int maxnb = 0;  // most bits any column of the group keeps
 #pragma unroll
             for (int c = 0; c < G; ++c) {
                 const int64_t j = g0 + 32 * c + lane;
@@ -137,12 +140,11 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
                 m[c] = in[c] ? __ldg(&t.mask[j]) : (U)0;
                 bv[c] = in[c] ? __ldg(&t.bitval[j]) : (U)0;
                 const int nb = in[c] ? (int)__ldg(&t.nb[j]) : 0;
-                few = few && nb <= 4;
+                maxnb = max(maxnb, nb);
                 cj[c] = in[c] && ((units[j >> 5] >> (j & 31)) & 1u);
-                len[c] = in[c] ? (cj[c] ? nb : W) : 0;
-                incl[c] = len[c];
+                incl[c] = in[c] ? (cj[c] ? nb : W) : 0;
             }
-            few = __all_sync(0xffffffffu, few);
+            maxnb = __reduce_max_sync(0xffffffffu, maxnb);
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
@@ -151,15 +153,17 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
                     if (lane >= o) incl[c] += y;
                 }
             }
-            int64_t cb = base;
-            if (few) {
-                // highly invariant columns: place each kept bit from the mask directly
-                // (at most 4 steps, no move-mask loads)
+            const U *gs = stream + (base >> LW);
+            const int32_t off0 = (int32_t)(base & (W - 1));
+            int32_t off = off0;
+            if (maxnb <= 4) {
+                // highly invariant columns: place each kept bit from the mask directly (at
+                // most 4 steps, no move-mask loads)
 #pragma unroll
                 for (int c = 0; c < G; ++c) {
                     const int64_t j = g0 + 32 * c + lane;
                     if (in[c]) {
-                        const U y = get_bits<U>(stream, cb + incl[c] - len[c], len[c]);
+                        const U y = stream_bits_ending<U>(gs, off + incl[c]);
                         U x = y;
                         if (cj[c]) {
                             U sel = (U)~m[c], r = 0;
@@ -173,21 +177,21 @@ __device__ __forceinline__ void decode_row(const U *__restrict__ buf, int64_t v,
                         }
                         orow[j] = x;
                     }
-                    cb += __shfl_sync(0xffffffffu, incl[c], 31);
+                    off += __shfl_sync(0xffffffffu, incl[c], 31);
                 }
             } else {
 #pragma unroll
                 for (int c = 0; c < G; ++c) {
                     const int64_t j = g0 + 32 * c + lane;
                     if (in[c]) {
-                        const U y = get_bits<U>(stream, cb + incl[c] - len[c], len[c]);
+                        const U y = stream_bits_ending<U>(gs, off + incl[c]);
                         orow[j] = cj[c] ? (U)(bv[c] | scatter_bits<U>(y, (U)~m[c], t.mv + j, (int)v))
                                         : y;
                     }
-                    cb += __shfl_sync(0xffffffffu, incl[c], 31);
+                    off += __shfl_sync(0xffffffffu, incl[c], 31);
                 }
             }
-            base = cb;
+            base += off - off0;
         }
     }
 }
