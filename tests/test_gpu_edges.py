@@ -253,6 +253,46 @@ def test_long_rows_longer_than_their_slot(ibp, oracle, wb, where):
     assert np.array_equal(ref, d[idx])
 
 
+@pytest.mark.parametrize("wb", [4, 8])
+@pytest.mark.parametrize("kept", [(1, 4), (5, 20)], ids=["few", "many"])
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_long_rows_few_and_many_kept_bits(ibp, wb, kept, where):
+    """Rows of 300 and 1100 words under masks that keep 1-4 bits per word (each kept bit
+    placed straight from the mask) or 5-20 (the move-mask scatter), with random values in
+    the kept bits, a few words stored whole and a few rows stored raw: whole sets and
+    batches decode to the source rows.  The first word of each row ends within the stream's
+    first word, so its read window starts in the row's bitmap."""
+    rng = np.random.default_rng(40 + wb + kept[0])
+    W = 8 * wb
+    it = {4: np.int32, 8: np.int64}[wb]
+    ut = {4: np.uint32, 8: np.uint64}[wb]
+    for v in (300, 1100):
+        n = 2000
+        keep = np.zeros(v, dtype=np.uint64)
+        for j in range(v):
+            for bit in rng.choice(W, rng.integers(kept[0], kept[1] + 1), replace=False):
+                keep[j] |= np.uint64(1) << np.uint64(bit)
+        keep = keep.astype(ut)
+        base = rng.integers(0, 2**63, v, dtype=np.uint64).astype(ut) & ~keep
+        noise = rng.integers(0, 2**63, (n, v), dtype=np.uint64).astype(ut)
+        data = (noise & keep) | base
+        whole = rng.random((n, v)) < 0.01
+        data = np.where(whole, noise, data)
+        data[rng.choice(n, 20, replace=False)] = noise[:20]
+        d = data.view(it)
+        m = torch.from_numpy((~keep).view(it)).cuda()
+        b = torch.from_numpy(base.view(it)).cuda()
+        x = torch.from_numpy(d.copy()).pin_memory()
+        cl = ibp.get_single_compress_len(x, m, b)
+        bm = ibp.compress_inplace(x, m, b)
+        xs = x if where == "host" else x.cuda()
+        idx = rng.integers(0, n, 700)
+        for ix in (None, idx):
+            ti = None if ix is None else torch.from_numpy(ix).cuda()
+            out = ibp.decompress_fetch(xs, m, b, bm, "cuda", cl, ti, check=True)
+            assert np.array_equal(out.cpu().numpy(), d if ix is None else d[ix])
+
+
 @pytest.mark.parametrize("wb,v", [(8, 64), (8, 65), (4, 131), (8, 600)])
 def test_device_rows_whole_set_and_small_batches(ibp, oracle, wb, v):
     """Device-resident rows of 512 bytes and up take the double-buffered read path; rows whose
